@@ -1,0 +1,140 @@
+/*
+ * dfttest2_b200 -- C ABI of the B200 (sm_100a) DFTTest per-plane hot path.
+ *
+ * The entry points replace the VapourSynth plugin functions of the
+ * reference's GPU backends (vs-dfttest2):
+ *
+ *   DFTTest  -> dfttest2_b200_create / dfttest2_b200_process_* / dfttest2_b200_free
+ *               (nvrtc_source/source.cpp:629-858 DFTTestCreate,
+ *                nvrtc_source/source.cpp:356-605 DFTTestGetFrame,
+ *                nvrtc_source/source.cpp:607-627 DFTTestFree,
+ *                signature registered at nvrtc_source/source.cpp:951-972)
+ *   RDFT     -> dfttest2_b200_rdft   (nvrtc_source/source.cpp:862-933,
+ *                                      cpu_source/source.cpp:269-340)
+ *   Version  -> dfttest2_b200_version (nvrtc_source/source.cpp:935-938)
+ *
+ * Only plain C types cross this boundary.  Every function that can fail
+ * returns 0 on success and a non-zero status otherwise; the message is
+ * available from dfttest2_b200_last_error() (thread-local) and uses the
+ * reference's wording where the reference has one.
+ *
+ * Array layouts are those of the plugin arguments: row-major (t, y, x),
+ * t in [0, 2*radius], y in [0, block_size), x in [0, block_size) for the
+ * window and x in [0, block_size/2] for sigma / window_freq; window_freq
+ * interleaves (re, im).
+ */
+#ifndef DFTTEST2_B200_H
+#define DFTTEST2_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DFTTEST2_B200_OK 0
+#define DFTTEST2_B200_EINVAL 1   /* invalid argument (same checks as the reference's Create) */
+#define DFTTEST2_B200_ECUDA 2    /* CUDA runtime error */
+#define DFTTEST2_B200_ENOMEM 3   /* allocation failure */
+#define DFTTEST2_B200_EKERNEL 4  /* the kernel reported an internal consistency failure */
+
+/* sample types, as VapourSynth's stInteger / stFloat */
+#define DFTTEST2_B200_INTEGER 0
+#define DFTTEST2_B200_FLOAT 1
+
+typedef struct dfttest2_b200_filter dfttest2_b200_filter;
+
+/* Arguments of DFTTest (nvrtc_source/source.cpp:951-972).  Integer options
+ * that the reference marks ":opt" take their reference default when set to
+ * -1 (radius 0, block_size 16, block_step block_size, zero_mean 1,
+ * device_id 0, num_streams 1). */
+typedef struct dfttest2_b200_params {
+    const double* window;      /* (2r+1)*B*B values */
+    int window_len;
+    const double* sigma;       /* 1 value (flat) or (2r+1)*B*(B/2+1) values */
+    int sigma_len;
+    double sigma2;
+    double pmin;
+    double pmax;
+    int filter_type;           /* 0..6 as translated by python/dfttest2.py:263-271 */
+    int radius;                /* 0..3 */
+    int block_size;            /* 8, 16 or 32 */
+    int block_step;
+    int zero_mean;
+    const double* window_freq; /* (2r+1)*B*(B/2+1)*2 values, required when zero_mean */
+    int window_freq_len;
+    int device_id;
+    int num_streams;
+    /* Temporal slice of `window` used as the synthesis window.  -1 selects the
+     * centre slice r, as dfttest2_nvrtc / dfttest2_cuda do
+     * (cuda_source/kernels.cu:240); dfttest2_cpu uses slice 2r
+     * (cpu_source/getframe_impl.cpp:383).  They agree for a rectangular
+     * temporal window or r = 0. */
+    int synthesis_slice;
+} dfttest2_b200_params;
+
+/* One output plane: 2r+1 source planes (frames n-r..n+r, already clamped to
+ * the clip as in nvrtc_source/source.cpp:427-431) and the destination.
+ * Strides are in bytes. */
+typedef struct dfttest2_b200_plane {
+    const void* src[7];
+    ptrdiff_t src_stride;
+    void* dst;
+    ptrdiff_t dst_stride;
+    int width;
+    int height;
+} dfttest2_b200_plane;
+
+/* Fills *p with the reference defaults (all optional fields -1). */
+void dfttest2_b200_params_init(dfttest2_b200_params* p);
+
+/* DFTTestCreate: validates the arguments, selects the device and uploads the
+ * constant tables.  On failure *out is NULL and the message is the
+ * reference's (e.g. "\"radius\" must be in [0, 1, 2, 3]"). */
+int dfttest2_b200_create(const dfttest2_b200_params* params, dfttest2_b200_filter** out);
+
+/* DFTTestFree */
+void dfttest2_b200_free(dfttest2_b200_filter* f);
+
+/* Batched device-resident path: every plane's pointers are device memory on
+ * the filter's device; all planes share the sample format.  The work is
+ * queued on `stream` (a cudaStream_t, NULL = legacy default stream) and the
+ * call returns without waiting.  This is the hot path that
+ * DFTTestGetFrame's kernel launches (nvrtc_source/source.cpp:487-551)
+ * correspond to, for any number of planes and frames at once. */
+int dfttest2_b200_process_planes(dfttest2_b200_filter* f, const dfttest2_b200_plane* planes, int nplanes,
+                                 int sample_type, int bits_per_sample, void* stream);
+
+/* Host-memory path with the semantics of DFTTestGetFrame for one plane:
+ * copies the 2r+1 source planes in, filters, copies the result out and
+ * waits for completion.  Concurrent calls are spread over num_streams
+ * stream slots (nvrtc_source/source.cpp:471-584). */
+int dfttest2_b200_process_plane_host(dfttest2_b200_filter* f, const dfttest2_b200_plane* plane, int sample_type,
+                                     int bits_per_sample);
+
+/* Whole-clip host path: filters `nframes` frames of one plane stored
+ * contiguously in host memory (frame i at src + i*frame_bytes, rows
+ * src_stride bytes apart) into dst.  Each source frame is uploaded once
+ * and reused by the 2r+1 outputs that need it; the temporal window is
+ * clamped at the clip ends (cpu_source/getframe_impl.cpp:296-298). */
+int dfttest2_b200_process_clip_host(dfttest2_b200_filter* f, const void* src, ptrdiff_t src_stride,
+                                    ptrdiff_t src_frame_bytes, void* dst, ptrdiff_t dst_stride,
+                                    ptrdiff_t dst_frame_bytes, int nframes, int width, int height, int sample_type,
+                                    int bits_per_sample);
+
+/* RDFT: FP64 direct real DFT over 1, 2 or 3 axes, real last axis first
+ * (cpu_source/source.cpp:269-340).  `out` receives
+ * prod(shape[:-1]) * (shape[-1]/2+1) interleaved (re, im) values. */
+int dfttest2_b200_rdft(const double* data, int data_len, const int* shape, int ndim, double* out, int out_len);
+
+/* Version string (version, build architecture, kernel variant). */
+const char* dfttest2_b200_version(void);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* dfttest2_b200_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DFTTEST2_B200_H */

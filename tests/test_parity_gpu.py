@@ -1,0 +1,201 @@
+"""Parity of the CUDA path (through the C ABI) with the reference.
+
+Bars (from the task's north star):
+* float32 planes: max-abs error <= 2e-5 of full scale (1.0);
+* 8/16-bit planes: within 1 LSB, exact-match fraction reported (and
+  required to stay high).
+Checked against: committed fixtures made with the reference's CPU math
+(tests/golden), the live reference build (oracle/_ref) when present, and
+the FP64 oracle (all block sizes).
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_planes, load_case, load_plane
+from dfttest2_b200.frontend import plugin_arguments
+from dfttest2_b200.plugin import Filter
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+FLOAT_TOL = 2e-5
+
+
+def sample_type_of(arr):
+    return 1 if arr.dtype == np.float32 else 0
+
+
+def gpu_plane(frames, args, bits, synthesis_slice=None, **extra):
+    flt = Filter(synthesis_slice=synthesis_slice, **args, **extra)
+    try:
+        return flt.process_plane_host(list(frames), sample_type_of(frames[0]), bits)
+    finally:
+        flt.close()
+
+
+def check(out, ref, bits, what=""):
+    """Returns the exact-match fraction; asserts the parity bar."""
+    if out.dtype == np.float32:
+        err = np.abs(out.astype(np.float64) - ref.astype(np.float64)).max()
+        assert err <= FLOAT_TOL, f"{what}: max-abs {err}"
+        return float(np.mean(out == ref))
+    d = np.abs(out.astype(np.int64) - ref.astype(np.int64))
+    assert d.max() <= 1, f"{what}: max diff {d.max()} LSB"
+    return float(np.mean(d == 0))
+
+
+@pytest.mark.parametrize("case", golden_planes())
+def test_golden_fixture(case, cuda_device):
+    rec, args = load_case(case)
+    frames, out_ref = load_plane(case)
+    out = gpu_plane(frames, args, rec["bits"], synthesis_slice=2 * args["radius"])
+    exact = check(out, out_ref, rec["bits"], case)
+    print(f"{case}: exact-match {exact:.4f}")
+    if out.dtype != np.float32:
+        assert exact >= 0.99
+
+
+def _frames(rng, n, h, w, dtype, bits):
+    x = np.clip(0.5 + 0.2 * rng.standard_normal((n, h, w)), 0, 1)
+    if dtype == np.float32:
+        return x.astype(np.float32)
+    return np.round(x * ((1 << bits) - 1)).astype(dtype)
+
+
+CONFIGS = [
+    # dtype, bits, tbsize, ftype, f0beta, swin, twin, sosize, zmean, (w, h)
+    (np.uint16, 16, 3, 0, 1.0, 0, 7, 12, True, (96, 72)),
+    (np.float32, 32, 3, 0, 1.0, 0, 7, 12, True, (71, 53)),
+    (np.uint8, 8, 1, 0, 1.0, 1, 7, 12, True, (64, 48)),
+    (np.uint16, 10, 5, 1, 1.0, 2, 7, 12, True, (100, 37)),
+    (np.float32, 32, 7, 0, 1.0, 3, 0, 12, True, (80, 64)),
+    (np.uint16, 16, 3, 2, 1.0, 4, 7, 8, False, (64, 64)),
+    (np.float32, 32, 3, 3, 1.0, 5, 7, 12, True, (90, 50)),
+    (np.uint8, 8, 5, 4, 1.0, 6, 9, 12, True, (77, 61)),
+    (np.uint16, 12, 3, 0, 0.7, 10, 7, 12, True, (64, 80)),
+    (np.float32, 32, 3, 0, 0.5, 11, 7, 4, True, (120, 66)),
+    (np.uint16, 16, 7, 0, 1.0, 0, 7, 12, False, (96, 96)),
+]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("cfg", CONFIGS, ids=[f"c{i}" for i in range(len(CONFIGS))])
+def test_against_reference_build(cfg, cuda_device):
+    dtype, bits, tb, ftype, f0, swin, twin, sosize, zm, (w, h) = cfg
+    rng = np.random.default_rng(tb * 7 + ftype + w)
+    frames = _frames(rng, tb, h, w, dtype, bits)
+    sigma = 0.9 if ftype in (2, 3, 4) else 6.0
+    args = plugin_arguments(ftype=ftype, f0beta=f0, sigma=sigma, sigma2=0.3, pmin=1.0, pmax=300.0, tbsize=tb,
+                            swin=swin, twin=twin, sosize=sosize, zmean=zm, full_sigma=True)
+    ref = O.ref_plane(list(frames), args, bits)
+    out = gpu_plane(frames, args, bits, synthesis_slice=2 * args["radius"])
+    exact = check(out, ref, bits, str(cfg))
+    print(f"cfg {cfg}: exact-match {exact:.4f}")
+
+
+@pytest.mark.parametrize("B,sosize,tb", [(8, 6, 1), (8, 6, 3), (8, 4, 5), (16, 12, 3), (32, 24, 1), (32, 16, 3),
+                                         (16, 8, 1), (32, 24, 5)])
+@pytest.mark.parametrize("dtype,bits", [(np.float32, 32), (np.uint16, 16)])
+def test_against_fp64_oracle(B, sosize, tb, dtype, bits, cuda_device):
+    rng = np.random.default_rng(B + tb)
+    w, h = 2 * B + 45, 2 * B + 27
+    frames = _frames(rng, tb, h, w, dtype, bits)
+    args = plugin_arguments(ftype=0, sigma=5.0, sbsize=B, sosize=sosize, tbsize=tb, swin=0, twin=7)
+    f64 = O.fp64_plane(list(frames), args, bits)
+    ref = O.quantize(f64, dtype, bits) if dtype != np.float32 else f64
+    out = gpu_plane(frames, args, bits)
+    exact = check(out, ref, bits, f"B{B} S{B - sosize} T{tb}")
+    print(f"B{B} T{tb} {dtype.__name__}: exact-match vs FP64 {exact:.4f}")
+
+
+def test_device_path_equals_host_path(cuda_device):
+    import torch
+    rng = np.random.default_rng(11)
+    clip = _frames(rng, 6, 72, 120, np.uint16, 16)
+    args = plugin_arguments(ftype=0, sigma=8.0, tbsize=3)
+    flt = Filter(**args)
+    try:
+        host = flt.process_clip_host(clip, 0, 16)
+        dev = flt.process_clip_device(torch.from_numpy(clip.view(np.int16)).cuda(), 0, 16)
+        torch.cuda.synchronize()
+        dev = dev.cpu().numpy().view(np.uint16)
+        per_plane = np.stack([flt.process_plane_host(O.clip_frames(clip, n, 1), 0, 16) for n in range(6)])
+    finally:
+        flt.close()
+    assert np.array_equal(host, dev)
+    assert np.abs(per_plane.astype(np.int64) - host.astype(np.int64)).max() <= 1
+
+
+def test_clip_end_clamp_matches_oracle(cuda_device):
+    rng = np.random.default_rng(5)
+    clip = _frames(rng, 4, 48, 64, np.float32, 32)
+    args = plugin_arguments(ftype=0, sigma=6.0, tbsize=5)
+    flt = Filter(**args)
+    try:
+        out = flt.process_clip_host(clip, 1, 32)
+    finally:
+        flt.close()
+    for n in range(4):
+        f64 = O.fp64_plane(O.clip_frames(clip, n, 2), args, 32)
+        check(out[n], f64, 32, f"frame {n}")
+
+
+def test_identity_full_hd_u16(cuda_device):
+    # multiplier 1 with zero-mean and a rectangular temporal window is the identity
+    import torch
+    rng = np.random.default_rng(0)
+    clip = _frames(rng, 3, 1080, 1920, np.uint16, 16)
+    args = plugin_arguments(ftype=2, sigma=1.0, tbsize=3)
+    flt = Filter(**args)
+    try:
+        dev = torch.from_numpy(clip.view(np.int16)).cuda()
+        out = flt.process_clip_device(dev, 0, 16)
+        torch.cuda.synchronize()
+        out = out.cpu().numpy().view(np.uint16)
+    finally:
+        flt.close()
+    d = np.abs(out.astype(np.int64) - clip.astype(np.int64))
+    assert d.max() <= 1
+    assert np.mean(d == 0) > 0.999
+
+
+def test_constant_plane_stays_constant(cuda_device):
+    clip = np.full((3, 540, 960), 1234, np.uint16)
+    args = plugin_arguments(ftype=0, sigma=8.0, tbsize=3)
+    flt = Filter(**args)
+    try:
+        out = flt.process_clip_host(clip, 0, 16)
+    finally:
+        flt.close()
+    assert np.abs(out.astype(np.int64) - 1234).max() <= 1
+
+
+def test_minimum_plane_and_too_small(cuda_device):
+    from dfttest2_b200._lib import Error
+    args = plugin_arguments(ftype=0, sigma=6.0, tbsize=3)
+    rng = np.random.default_rng(9)
+    # 16x16 pads by 12 on each side (ox = oy = 12 < 16)
+    frames = _frames(rng, 3, 16, 16, np.float32, 32)
+    out = gpu_plane(frames, args, 32)
+    f64 = O.fp64_plane(list(frames), args, 32)
+    check(out, f64, 32, "16x16")
+    with pytest.raises(Error, match="too small"):
+        gpu_plane(_frames(rng, 3, 12, 40, np.float32, 32), args, 32)
+
+
+def test_batch_of_planes_matches_single_launches(cuda_device):
+    """Many planes in one launch (whole-height strips) vs one plane per launch
+    (strips split into segments; shared zones summed by the fix-up)."""
+    rng = np.random.default_rng(21)
+    clip = _frames(rng, 12, 270, 480, np.uint16, 16)
+    args = plugin_arguments(ftype=0, sigma=8.0, tbsize=3)
+    flt = Filter(**args)
+    try:
+        batch = flt.process_clip_host(clip, 0, 16)
+        singles = np.stack([flt.process_plane_host(O.clip_frames(clip, n, 1), 0, 16) for n in (0, 5, 11)])
+    finally:
+        flt.close()
+    d = np.abs(batch[[0, 5, 11]].astype(np.int64) - singles.astype(np.int64))
+    assert d.max() <= 1
+    f64 = O.fp64_plane(O.clip_frames(clip, 5, 1), args, 16)
+    check(batch[5], O.quantize(f64, np.uint16, 16), 16, "batch frame 5")

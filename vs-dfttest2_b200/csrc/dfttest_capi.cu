@@ -1,0 +1,726 @@
+// C ABI of the B200 DFTTest hot path (declared in include/dfttest2_b200.h).
+//
+// Host responsibilities, mirroring the reference's plugin glue:
+//   * argument validation with the reference's messages
+//     (nvrtc_source/source.cpp:629-858),
+//   * conversion of the FP64 plugin arrays to the FP32 tables the kernel
+//     reads (window, per-gain-slot sigma and window spectrum),
+//   * splitting every plane into units, sizing the per-unit scratch,
+//   * stream slots for concurrent callers (nvrtc_source/source.cpp:272-291),
+//   * the host-memory paths and RDFT (cpu_source/source.cpp:269-340).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <complex>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "dfttest2_b200.h"
+#include "dfttest_kernel.cuh"
+
+#ifndef DFTTEST2_B200_VERSION
+#define DFTTEST2_B200_VERSION "0.1.0"
+#endif
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                                   \
+    do {                                                                                                 \
+        cudaError_t e_ = (expr);                                                                         \
+        if (e_ != cudaSuccess) {                                                                         \
+            return fail(DFTTEST2_B200_ECUDA, std::string("[") + std::to_string(__LINE__) + "] '" #expr   \
+                                                 "' failed: " + cudaGetErrorString(e_));                 \
+        }                                                                                                \
+    } while (0)
+
+using KernelFn = void (*)(const dft2::KernelArgs);
+
+struct Variant {
+    KernelFn main = nullptr;
+    KernelFn fixup = nullptr;
+    int nw = 0;      // warps per CTA
+    int bpw = 0;     // blocks per warp
+    size_t (*smem)(int pitch) = nullptr;
+};
+
+template <int B, int T, int NW>
+Variant make_variant() {
+    Variant v;
+    v.main = dft2::dfttest_unit_kernel<B, T, NW>;
+    v.fixup = dft2::dfttest_fixup_kernel<B>;
+    v.nw = NW;
+    v.bpw = 64 / B;
+    v.smem = [](int pitch) { return dft2::Layout<B, T, NW>::smem_bytes(pitch); };
+    return v;
+}
+
+// kernel variants per (block size, temporal size); NW keeps the per-warp
+// buffers plus rings within the shared-memory budget
+Variant select_variant(int B, int T) {
+    switch (B) {
+#ifndef DFTTEST2_B200_ONLY_B16
+    case 8:
+        switch (T) {
+        case 1: return make_variant<8, 1, 8>();
+        case 3: return make_variant<8, 3, 8>();
+        case 5: return make_variant<8, 5, 8>();
+        case 7: return make_variant<8, 7, 8>();
+        }
+        break;
+#endif
+    case 16:
+        switch (T) {
+        case 1: return make_variant<16, 1, 8>();
+        case 3: return make_variant<16, 3, 8>();
+        case 5: return make_variant<16, 5, 4>();
+        case 7: return make_variant<16, 7, 4>();
+        }
+        break;
+#ifndef DFTTEST2_B200_ONLY_B16
+    case 32:
+        switch (T) {
+        case 1: return make_variant<32, 1, 8>();
+        case 3: return make_variant<32, 3, 4>();
+        case 5: return make_variant<32, 5, 2>();
+        case 7: return make_variant<32, 7, 2>();
+        }
+        break;
+#endif
+    }
+    return Variant{};
+}
+
+struct Slot {
+    cudaEvent_t done = nullptr;
+    cudaStream_t stream = nullptr;        // own stream (host paths)
+    dft2::PlaneJob* d_jobs = nullptr;
+    size_t jobs_cap = 0;
+    float* d_scratch = nullptr;
+    size_t scratch_cap = 0;               // floats
+    int* d_error = nullptr;
+    // host path staging
+    void* d_frames = nullptr;
+    size_t frames_cap = 0;
+    void* h_pinned = nullptr;
+    size_t pinned_cap = 0;
+};
+
+}  // namespace
+
+struct dfttest2_b200_filter {
+    int device = 0;
+    int radius = 0, T = 1, B = 16, S = 16, H = 8;
+    int filter_type = 0;
+    bool zero_mean = true;
+    float sigma2 = 0, pmin = 0, pmax = 0;
+    int syn_slice = 0;
+    float g_div = 0.0f;
+    bool asym = false;
+    Variant var;
+    int num_sms = 148;
+
+    float* d_win = nullptr;
+    float* d_wsyn = nullptr;
+    float* d_sig = nullptr;
+    float* d_sig2 = nullptr;
+    float* d_wfe = nullptr;
+
+    std::vector<Slot> slots;
+    std::vector<int> free_slots;
+    std::mutex slot_lock;
+    std::condition_variable slot_cv;
+};
+
+namespace {
+
+struct SlotGuard {
+    dfttest2_b200_filter* f;
+    int idx;
+    SlotGuard(dfttest2_b200_filter* f_) : f(f_) {
+        std::unique_lock<std::mutex> lk(f->slot_lock);
+        f->slot_cv.wait(lk, [&] { return !f->free_slots.empty(); });
+        idx = f->free_slots.back();
+        f->free_slots.pop_back();
+    }
+    ~SlotGuard() {
+        {
+            std::lock_guard<std::mutex> lk(f->slot_lock);
+            f->free_slots.push_back(idx);
+        }
+        f->slot_cv.notify_one();
+    }
+    Slot& slot() { return f->slots[idx]; }
+};
+
+// grows a device buffer after the slot's previous work has finished
+template <typename Tp>
+int ensure(Tp*& ptr, size_t& cap, size_t need, cudaEvent_t done) {
+    if (need <= cap) return 0;
+    CUDA_TRY(cudaEventSynchronize(done));
+    if (ptr) CUDA_TRY(cudaFree(ptr));
+    ptr = nullptr;
+    cap = 0;
+    size_t n = std::max(need, cap * 2);
+    if (cudaMalloc((void**)&ptr, n * sizeof(Tp)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DFTTEST2_B200_ENOMEM, "device allocation failed");
+    }
+    cap = n;
+    return 0;
+}
+
+int ensure_bytes(void*& ptr, size_t& cap, size_t need, cudaEvent_t done) {
+    if (need <= cap) return 0;
+    CUDA_TRY(cudaEventSynchronize(done));
+    if (ptr) CUDA_TRY(cudaFree(ptr));
+    ptr = nullptr;
+    cap = 0;
+    if (cudaMalloc(&ptr, need) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DFTTEST2_B200_ENOMEM, "device allocation failed");
+    }
+    cap = need;
+    return 0;
+}
+
+int ensure_pinned(void*& ptr, size_t& cap, size_t need, cudaEvent_t done) {
+    if (need <= cap) return 0;
+    CUDA_TRY(cudaEventSynchronize(done));
+    if (ptr) CUDA_TRY(cudaFreeHost(ptr));
+    ptr = nullptr;
+    cap = 0;
+    if (cudaMallocHost(&ptr, need) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DFTTEST2_B200_ENOMEM, "pinned host allocation failed");
+    }
+    cap = need;
+    return 0;
+}
+
+int bytes_of(int sample_type, int bits) {
+    if (sample_type == DFTTEST2_B200_FLOAT) return 4;
+    return bits <= 8 ? 1 : 2;
+}
+
+int check_format(int sample_type, int bits) {
+    if (sample_type == DFTTEST2_B200_INTEGER) {
+        if (bits < 8 || bits > 16) return fail(DFTTEST2_B200_EINVAL, "only 8-16 bit integer format input is supported");
+        return 0;
+    }
+    if (sample_type == DFTTEST2_B200_FLOAT && bits == 32) return 0;
+    return fail(DFTTEST2_B200_EINVAL, "only 8-16 bit integer and 32-bit float format input is supported");
+}
+
+// planning of one launch over a list of planes
+struct Plan {
+    std::vector<dft2::PlaneJob> jobs;
+    int nunits = 0;
+    int nfix = 0;
+    int rec_stride = 0;
+    int pitch = 0;
+};
+
+int make_plan(const dfttest2_b200_filter* f, const dfttest2_b200_plane* planes, int n, int bps_bytes, Plan& plan) {
+    const int B = f->B, S = f->S, O = B - S;
+    const int BPS = f->var.nw * f->var.bpw;
+    plan.jobs.resize(n);
+    // strips: BPS blocks at most; segments only when the launch is small
+    long long strips_total = 0;
+    int max_pny = 0;
+    for (int i = 0; i < n; ++i) {
+        const dfttest2_b200_plane& p = planes[i];
+        const int pw = dft2::pad_size(p.width, B, S), ph = dft2::pad_size(p.height, B, S);
+        const int ox = (pw - p.width) / 2, oy = (ph - p.height) / 2;
+        // the mirror padding must stay inside the plane
+        // (cpu_source/getframe_impl.cpp:44-62 reads 2*ox - x)
+        if (p.width <= std::max(ox, pw - p.width - ox) || p.height <= std::max(oy, ph - p.height - oy))
+            return fail(DFTTEST2_B200_EINVAL, "plane too small for the block size");
+        const int pnx = dft2::pad_num(p.width, B, S);
+        strips_total += (pnx + BPS - 1) / BPS;
+        max_pny = std::max(max_pny, dft2::pad_num(p.height, B, S));
+        for (int t = 0; t < f->T; ++t) {
+            if (p.src[t] == nullptr) return fail(DFTTEST2_B200_EINVAL, "null source plane");
+        }
+        if (!p.dst) return fail(DFTTEST2_B200_EINVAL, "null destination plane");
+        if (p.src_stride % bps_bytes || p.dst_stride % bps_bytes || p.src_stride < (ptrdiff_t)p.width * bps_bytes ||
+            p.dst_stride < (ptrdiff_t)p.width * bps_bytes)
+            return fail(DFTTEST2_B200_EINVAL, "invalid stride");
+    }
+    const long long target = 4LL * f->num_sms;
+    int nsy = 1;
+    if (strips_total < target) nsy = (int)((target + strips_total - 1) / strips_total);
+    const int min_seg = std::max((O + S - 1) / S, 4);
+    nsy = std::max(1, std::min(nsy, max_pny / min_seg));
+
+    int unit = 0, fix = 0, rec = 0;
+    for (int i = 0; i < n; ++i) {
+        const dfttest2_b200_plane& p = planes[i];
+        dft2::PlaneJob& j = plan.jobs[i];
+        std::memset(&j, 0, sizeof(j));
+        for (int t = 0; t < f->T; ++t) j.src[t] = p.src[t];
+        j.dst = p.dst;
+        j.src_stride = p.src_stride / bps_bytes;
+        j.dst_stride = p.dst_stride / bps_bytes;
+        j.width = p.width;
+        j.height = p.height;
+        const int pnx = dft2::pad_num(p.width, B, S), pny = dft2::pad_num(p.height, B, S);
+        j.nsx = (pnx + BPS - 1) / BPS;
+        j.nsy = std::max(1, std::min(nsy, pny / min_seg));
+        // strips must be at least O/S blocks wide so that bands do not overlap
+        while (j.nsx > 1 && pnx / j.nsx < (O + S - 1) / S) --j.nsx;
+        j.unit_base = unit;
+        j.fix_base = fix;
+        unit += j.nsx * j.nsy;
+        fix += (j.nsx - 1) * O * p.height + (j.nsy - 1) * O * p.width;
+        const int wmax = (pnx + j.nsx - 1) / j.nsx, hmax = (pny + j.nsy - 1) / j.nsy;
+        rec = std::max(rec, dft2::band_record_size(wmax * S + O, hmax * S + O, O));
+    }
+    plan.nunits = unit;
+    plan.nfix = fix;
+    plan.rec_stride = std::max(rec, 1);
+    plan.pitch = ((BPS * S + O) + 3) & ~3;
+    return 0;
+}
+
+int launch(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, float scale, float peak,
+           cudaStream_t stream) {
+    if (plan.nunits == 0) return 0;
+    CUDA_TRY(cudaStreamWaitEvent(stream, slot.done, 0));
+    if (int rc = ensure(slot.d_jobs, slot.jobs_cap, plan.jobs.size(), slot.done)) return rc;
+    const size_t scratch_need = (size_t)plan.nunits * plan.rec_stride;
+    if (int rc = ensure(slot.d_scratch, slot.scratch_cap, scratch_need, slot.done)) return rc;
+    CUDA_TRY(cudaMemcpyAsync(slot.d_jobs, plan.jobs.data(), plan.jobs.size() * sizeof(dft2::PlaneJob),
+                             cudaMemcpyHostToDevice, stream));
+
+    dft2::KernelArgs a{};
+    a.jobs = slot.d_jobs;
+    a.njobs = (int)plan.jobs.size();
+    a.nunits = plan.nunits;
+    a.nfix = plan.nfix;
+    a.kind = kind;
+    a.scale = scale;
+    a.peak = peak;
+    a.block_step = f->S;
+    a.filter_type = f->filter_type;
+    a.sigma2 = f->sigma2;
+    a.pmin = f->pmin;
+    a.pmax = f->pmax;
+    a.g_div = f->zero_mean ? f->g_div : 0.0f;
+    a.win = f->d_win;
+    a.wsyn = f->d_wsyn;
+    a.sig = f->d_sig;
+    a.sig2 = f->asym ? f->d_sig2 : nullptr;
+    a.wfe = f->d_wfe;
+    a.scratch = slot.d_scratch;
+    a.rec_stride = plan.rec_stride;
+    a.ring_pitch = plan.pitch;
+    a.error_flag = slot.d_error;
+
+    const size_t smem = f->var.smem(plan.pitch);
+    CUDA_TRY(cudaFuncSetAttribute(f->var.main, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    f->var.main<<<plan.nunits, f->var.nw * 32, smem, stream>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    if (plan.nfix > 0) {
+        const int threads = 256;
+        const int blocks = std::min((plan.nfix + threads - 1) / threads, f->num_sms * 8);
+        f->var.fixup<<<blocks, threads, 0, stream>>>(a);
+        CUDA_TRY(cudaGetLastError());
+    }
+    CUDA_TRY(cudaEventRecord(slot.done, stream));
+    return 0;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+void scale_peak(int sample_type, int bits, float& scale, float& peak, int& kind) {
+    if (sample_type == DFTTEST2_B200_FLOAT) {
+        scale = 255.0f;
+        peak = 1.0f;
+        kind = dft2::kF32;
+    } else {
+        scale = 1.0f / (float)(1 << (bits - 8));
+        peak = (float)((1 << bits) - 1);
+        kind = bits <= 8 ? dft2::kU8 : dft2::kU16;
+    }
+}
+
+void free_filter(dfttest2_b200_filter* f) {
+    if (!f) return;
+    DeviceGuard g(f->device);
+    for (Slot& s : f->slots) {
+        if (s.done) cudaEventSynchronize(s.done);
+        if (s.d_jobs) cudaFree(s.d_jobs);
+        if (s.d_scratch) cudaFree(s.d_scratch);
+        if (s.d_error) cudaFree(s.d_error);
+        if (s.d_frames) cudaFree(s.d_frames);
+        if (s.h_pinned) cudaFreeHost(s.h_pinned);
+        if (s.stream) cudaStreamDestroy(s.stream);
+        if (s.done) cudaEventDestroy(s.done);
+    }
+    cudaFree(f->d_win);
+    cudaFree(f->d_wsyn);
+    cudaFree(f->d_sig);
+    cudaFree(f->d_sig2);
+    cudaFree(f->d_wfe);
+    delete f;
+}
+
+template <typename Tp>
+int upload(Tp*& dptr, const std::vector<Tp>& h) {
+    CUDA_TRY(cudaMalloc((void**)&dptr, std::max<size_t>(h.size(), 1) * sizeof(Tp)));
+    if (!h.empty()) CUDA_TRY(cudaMemcpy(dptr, h.data(), h.size() * sizeof(Tp), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+void dfttest2_b200_params_init(dfttest2_b200_params* p) {
+    std::memset(p, 0, sizeof(*p));
+    p->radius = -1;
+    p->block_size = -1;
+    p->block_step = -1;
+    p->zero_mean = -1;
+    p->device_id = -1;
+    p->num_streams = -1;
+    p->synthesis_slice = -1;
+}
+
+int dfttest2_b200_create(const dfttest2_b200_params* p, dfttest2_b200_filter** out) {
+    if (!out) return fail(DFTTEST2_B200_EINVAL, "null output handle");
+    *out = nullptr;
+    if (!p) return fail(DFTTEST2_B200_EINVAL, "null parameters");
+    const int radius = p->radius < 0 ? 0 : p->radius;
+    if (p->radius > 3) return fail(DFTTEST2_B200_EINVAL, "\"radius\" must be in [0, 1, 2, 3]");
+    const int B = p->block_size < 0 ? 16 : p->block_size;
+    if (B != 8 && B != 16 && B != 32) return fail(DFTTEST2_B200_EINVAL, "\"block_size\" must be 8, 16 or 32");
+    const int S = p->block_step < 0 ? B : p->block_step;
+    if (S < 1 || S > B) return fail(DFTTEST2_B200_EINVAL, "\"block_step\" must be in [1, block_size]");
+    const int T = 2 * radius + 1, H = B / 2, X = H + 1;
+    const int zero_mean = p->zero_mean < 0 ? 1 : !!p->zero_mean;
+    const int device_id = p->device_id < 0 ? 0 : p->device_id;
+    const int num_streams = p->num_streams < 0 ? 1 : p->num_streams;
+    if (num_streams < 1) return fail(DFTTEST2_B200_EINVAL, "\"num_streams\" must be positive");
+    if (p->filter_type < 0 || p->filter_type > 6) return fail(DFTTEST2_B200_EINVAL, "\"filter_type\" must be in [0, 6]");
+
+    if (p->window_len != T * B * B || !p->window) return fail(DFTTEST2_B200_EINVAL, "invalid window size");
+    if (p->sigma_len <= 0 || !p->sigma) return fail(DFTTEST2_B200_EINVAL, "sigma must not be empty");
+    if (p->sigma_len != 1 && p->sigma_len != T * B * X) return fail(DFTTEST2_B200_EINVAL, "invalid sigma array size");
+    if (zero_mean && (p->window_freq_len != T * B * X * 2 || !p->window_freq))
+        return fail(DFTTEST2_B200_EINVAL, "invalid window_freq size");
+    const int syn = p->synthesis_slice < 0 ? radius : p->synthesis_slice;
+    if (syn >= T) return fail(DFTTEST2_B200_EINVAL, "\"synthesis_slice\" out of range");
+
+    std::unique_ptr<dfttest2_b200_filter, void (*)(dfttest2_b200_filter*)> f(new dfttest2_b200_filter, free_filter);
+    f->device = device_id;
+    f->radius = radius;
+    f->T = T;
+    f->B = B;
+    f->S = S;
+    f->H = H;
+    f->filter_type = p->filter_type;
+    f->zero_mean = zero_mean;
+    f->sigma2 = (float)p->sigma2;
+    f->pmin = (float)p->pmin;
+    f->pmax = (float)p->pmax;
+    f->syn_slice = syn;
+    f->var = select_variant(B, T);
+    if (!f->var.main) return fail(DFTTEST2_B200_EINVAL, "unsupported block_size / radius");
+
+    // -- tables --------------------------------------------------------------
+    std::vector<float> win(T * B * B), wsyn(B * B);
+    for (int i = 0; i < T * B * B; ++i) win[i] = (float)p->window[i];
+    for (int i = 0; i < B * B; ++i) wsyn[i] = win[syn * B * B + i];
+    auto sigma_at = [&](int t, int y, int x) -> float {
+        return p->sigma_len == 1 ? (float)p->sigma[0] : (float)p->sigma[(t * B + y) * X + x];
+    };
+    auto wf_at = [&](int t, int y, int x, int part) -> float {
+        if (!zero_mean) return 0.0f;
+        return (float)p->window_freq[((t * B + y) * X + x) * 2 + part];
+    };
+    const int NS = B + 2;
+    std::vector<float> sig(T * NS * H), sig2(T * NS * H), wfe(2 * T * NS * H);
+    bool asym = false;
+    // gain slot j of plane p for lane column c -> spectrum bin (t, y, x) and
+    // the Hermitian partner bin of the packed columns
+    auto put = [&](int pl, int j, int c, int t, int y, int x, int t2, int y2) {
+        const int idx = (pl * NS + j) * H + c;
+        sig[idx] = sigma_at(t, y, x);
+        sig2[idx] = sigma_at(t2, y2, x);
+        wfe[2 * idx] = wf_at(t, y, x, 0);
+        wfe[2 * idx + 1] = wf_at(t, y, x, 1);
+        if (sig2[idx] != sig[idx]) asym = true;
+    };
+    for (int pl = 0; pl < T; ++pl) {
+        for (int c = 0; c < H; ++c) {
+            if (pl == 0) {
+                for (int j = 0; j < B; ++j) {
+                    const int k = j >> 1;
+                    if (c > 0) {
+                        const int y = j == 0 ? 0 : (j == 1 ? H : ((j & 1) ? B - k : k));
+                        put(0, j, c, 0, y, c, 0, y);
+                    } else {
+                        // packed plane 0: A (x=0) at even slots, B (x=H) at odd slots
+                        const int ky = (j < 2) ? 0 : k;
+                        const int x = (j & 1) ? H : 0;
+                        put(0, j, 0, 0, ky, x, 0, (B - ky) % B);
+                    }
+                }
+                // extra packed slots: Nyquist-y bins of columns 0 and H
+                put(0, B, c, 0, H, 0, 0, H);
+                put(0, B + 1, c, 0, H, H, 0, H);
+            } else {
+                for (int y = 0; y < B; ++y) {
+                    if (c > 0) {
+                        put(pl, y, c, pl, y, c, pl, y);
+                    } else if (pl <= radius) {
+                        put(pl, y, 0, pl, y, 0, T - pl, (B - y) % B);
+                    } else {
+                        put(pl, y, 0, T - pl, y, H, pl, (B - y) % B);
+                    }
+                }
+                put(pl, B, c, 0, 0, 0, 0, 0);
+                put(pl, B + 1, c, 0, 0, 0, 0, 0);
+            }
+        }
+    }
+    f->asym = asym;
+    f->g_div = zero_mean ? (float)p->window_freq[0] : 0.0f;
+    if (zero_mean && f->g_div == 0.0f) return fail(DFTTEST2_B200_EINVAL, "window_freq[0] must be non-zero");
+
+    int ndev = 0;
+    CUDA_TRY(cudaGetDeviceCount(&ndev));
+    if (device_id >= ndev) return fail(DFTTEST2_B200_EINVAL, "invalid device_id");
+    DeviceGuard dg(device_id);
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, device_id));
+    if (prop.major < 10) return fail(DFTTEST2_B200_EINVAL, "device is not sm_100 class");
+    f->num_sms = prop.multiProcessorCount;
+
+    if (int rc = upload(f->d_win, win)) return rc;
+    if (int rc = upload(f->d_wsyn, wsyn)) return rc;
+    if (int rc = upload(f->d_sig, sig)) return rc;
+    if (int rc = upload(f->d_sig2, sig2)) return rc;
+    if (int rc = upload(f->d_wfe, wfe)) return rc;
+
+    f->slots.resize(num_streams);
+    for (int i = 0; i < num_streams; ++i) {
+        Slot& s = f->slots[i];
+        CUDA_TRY(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+        CUDA_TRY(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaMalloc((void**)&s.d_error, sizeof(int)));
+        CUDA_TRY(cudaMemset(s.d_error, 0, sizeof(int)));
+        CUDA_TRY(cudaEventRecord(s.done, s.stream));
+        f->free_slots.push_back(i);
+    }
+    CUDA_TRY(cudaDeviceSynchronize());
+    *out = f.release();
+    g_last_error.clear();
+    return 0;
+}
+
+void dfttest2_b200_free(dfttest2_b200_filter* f) { free_filter(f); }
+
+int dfttest2_b200_process_planes(dfttest2_b200_filter* f, const dfttest2_b200_plane* planes, int nplanes,
+                                 int sample_type, int bits_per_sample, void* stream) {
+    if (!f) return fail(DFTTEST2_B200_EINVAL, "null filter");
+    if (nplanes < 0 || (nplanes > 0 && !planes)) return fail(DFTTEST2_B200_EINVAL, "invalid plane list");
+    if (int rc = check_format(sample_type, bits_per_sample)) return rc;
+    DeviceGuard dg(f->device);
+    Plan plan;
+    if (int rc = make_plan(f, planes, nplanes, bytes_of(sample_type, bits_per_sample), plan)) return rc;
+    float scale, peak;
+    int kind;
+    scale_peak(sample_type, bits_per_sample, scale, peak, kind);
+    SlotGuard sg(f);
+    return launch(f, sg.slot(), plan, kind, scale, peak, (cudaStream_t)stream);
+}
+
+int dfttest2_b200_process_plane_host(dfttest2_b200_filter* f, const dfttest2_b200_plane* plane, int sample_type,
+                                     int bits_per_sample) {
+    if (!f || !plane) return fail(DFTTEST2_B200_EINVAL, "null argument");
+    if (int rc = check_format(sample_type, bits_per_sample)) return rc;
+    DeviceGuard dg(f->device);
+    const int bps = bytes_of(sample_type, bits_per_sample);
+    const size_t row = (size_t)plane->width * bps;
+    const size_t frame = row * plane->height;
+    const int T = f->T;
+    SlotGuard sg(f);
+    Slot& s = sg.slot();
+    // T input planes + 1 output plane, densely packed
+    if (int rc = ensure_bytes(s.d_frames, s.frames_cap, frame * (T + 1), s.done)) return rc;
+    if (int rc = ensure_pinned(s.h_pinned, s.pinned_cap, frame * (T + 1), s.done)) return rc;
+    CUDA_TRY(cudaEventSynchronize(s.done));
+    uint8_t* h = (uint8_t*)s.h_pinned;
+    for (int t = 0; t < T; ++t) {
+        const uint8_t* src = (const uint8_t*)plane->src[t];
+        if (!src) return fail(DFTTEST2_B200_EINVAL, "null source plane");
+        for (int y = 0; y < plane->height; ++y) std::memcpy(h + t * frame + y * row, src + y * plane->src_stride, row);
+    }
+    CUDA_TRY(cudaMemcpyAsync(s.d_frames, h, frame * T, cudaMemcpyHostToDevice, s.stream));
+    dfttest2_b200_plane dp{};
+    for (int t = 0; t < T; ++t) dp.src[t] = (uint8_t*)s.d_frames + t * frame;
+    dp.src_stride = row;
+    dp.dst = (uint8_t*)s.d_frames + T * frame;
+    dp.dst_stride = row;
+    dp.width = plane->width;
+    dp.height = plane->height;
+    Plan plan;
+    if (int rc = make_plan(f, &dp, 1, bps, plan)) return rc;
+    float scale, peak;
+    int kind;
+    scale_peak(sample_type, bits_per_sample, scale, peak, kind);
+    if (int rc = launch(f, s, plan, kind, scale, peak, s.stream)) return rc;
+    CUDA_TRY(cudaMemcpyAsync(h + T * frame, dp.dst, frame, cudaMemcpyDeviceToHost, s.stream));
+    CUDA_TRY(cudaEventRecord(s.done, s.stream));
+    CUDA_TRY(cudaEventSynchronize(s.done));
+    uint8_t* dst = (uint8_t*)plane->dst;
+    for (int y = 0; y < plane->height; ++y) std::memcpy(dst + y * plane->dst_stride, h + T * frame + y * row, row);
+    return 0;
+}
+
+int dfttest2_b200_process_clip_host(dfttest2_b200_filter* f, const void* src, ptrdiff_t src_stride,
+                                    ptrdiff_t src_frame_bytes, void* dst, ptrdiff_t dst_stride,
+                                    ptrdiff_t dst_frame_bytes, int nframes, int width, int height, int sample_type,
+                                    int bits_per_sample) {
+    if (!f || !src || !dst || nframes <= 0) return fail(DFTTEST2_B200_EINVAL, "invalid argument");
+    if (int rc = check_format(sample_type, bits_per_sample)) return rc;
+    DeviceGuard dg(f->device);
+    const int bps = bytes_of(sample_type, bits_per_sample);
+    const size_t row = (size_t)width * bps;
+    const size_t frame = row * height;
+    const int r = f->radius;
+    SlotGuard sg(f);
+    Slot& s = sg.slot();
+    // chunked pipeline: every source frame is uploaded once into a dense
+    // device array; a chunk of outputs is filtered with one launch
+    const int chunk = std::max(1, std::min(nframes, 32));
+    if (int rc = ensure_bytes(s.d_frames, s.frames_cap, frame * ((size_t)nframes + chunk), s.done)) return rc;
+    CUDA_TRY(cudaEventSynchronize(s.done));
+    uint8_t* dframes = (uint8_t*)s.d_frames;
+    uint8_t* dout = dframes + frame * nframes;
+    const uint8_t* hsrc = (const uint8_t*)src;
+    uint8_t* hdst = (uint8_t*)dst;
+    float scale, peak;
+    int kind;
+    scale_peak(sample_type, bits_per_sample, scale, peak, kind);
+    int uploaded = 0;
+    for (int c0 = 0; c0 < nframes; c0 += chunk) {
+        const int c1 = std::min(nframes, c0 + chunk);
+        const int need = std::min(nframes, c1 + r);
+        for (; uploaded < need; ++uploaded) {
+            CUDA_TRY(cudaMemcpy2DAsync(dframes + frame * uploaded, row, hsrc + src_frame_bytes * uploaded, src_stride,
+                                       row, height, cudaMemcpyHostToDevice, s.stream));
+        }
+        std::vector<dfttest2_b200_plane> planes(c1 - c0);
+        for (int n = c0; n < c1; ++n) {
+            dfttest2_b200_plane& p = planes[n - c0];
+            std::memset(&p, 0, sizeof(p));
+            for (int t = 0; t < f->T; ++t) {
+                const int fi = std::min(std::max(n - r + t, 0), nframes - 1);
+                p.src[t] = dframes + frame * fi;
+            }
+            p.src_stride = row;
+            p.dst = dout + frame * (n - c0);
+            p.dst_stride = row;
+            p.width = width;
+            p.height = height;
+        }
+        Plan plan;
+        if (int rc = make_plan(f, planes.data(), (int)planes.size(), bps, plan)) return rc;
+        if (int rc = launch(f, s, plan, kind, scale, peak, s.stream)) return rc;
+        for (int n = c0; n < c1; ++n) {
+            CUDA_TRY(cudaMemcpy2DAsync(hdst + dst_frame_bytes * n, dst_stride, dout + frame * (n - c0), row, row,
+                                       height, cudaMemcpyDeviceToHost, s.stream));
+        }
+        CUDA_TRY(cudaEventRecord(s.done, s.stream));
+        CUDA_TRY(cudaEventSynchronize(s.done));
+    }
+    return 0;
+}
+
+int dfttest2_b200_rdft(const double* data, int data_len, const int* shape, int ndim, double* out, int out_len) {
+    if (ndim != 1 && ndim != 2 && ndim != 3)
+        return fail(DFTTEST2_B200_EINVAL, "\"shape\" must be an array of ints with 1, 2 or 3 values");
+    if (!data || !shape || !out) return fail(DFTTEST2_B200_EINVAL, "null argument");
+    long long size = 1;
+    for (int i = 0; i < ndim; ++i) {
+        if (shape[i] <= 0) return fail(DFTTEST2_B200_EINVAL, "cannot reshape array");
+        size *= shape[i];
+    }
+    if (size != data_len) return fail(DFTTEST2_B200_EINVAL, "cannot reshape array");
+    const int nx = shape[ndim - 1], xo = nx / 2 + 1;
+    long long outer = size / nx;
+    if ((long long)out_len != outer * xo * 2) return fail(DFTTEST2_B200_EINVAL, "invalid output size");
+    using C = std::complex<double>;
+    const double pi = 3.14159265358979323846;
+    // real last axis first, then the remaining axes from the innermost out
+    std::vector<C> buf(outer * xo);
+    for (long long o = 0; o < outer; ++o) {
+        for (int k = 0; k < xo; ++k) {
+            C sum = 0.0;
+            for (int j = 0; j < nx; ++j) {
+                const double ang = -2.0 * pi * (double)k * j / nx;
+                sum += data[o * nx + j] * C(std::cos(ang), std::sin(ang));
+            }
+            buf[o * xo + k] = sum;
+        }
+    }
+    long long inner = xo;  // stride of the axis being transformed
+    for (int ax = ndim - 2; ax >= 0; --ax) {
+        const int n = shape[ax];
+        const long long block = inner * n;
+        std::vector<C> tmp(buf.size());
+        for (long long base = 0; base < (long long)buf.size(); base += block) {
+            for (long long in = 0; in < inner; ++in) {
+                for (int k = 0; k < n; ++k) {
+                    C sum = 0.0;
+                    for (int j = 0; j < n; ++j) {
+                        const double ang = -2.0 * pi * (double)k * j / n;
+                        sum += buf[base + j * inner + in] * C(std::cos(ang), std::sin(ang));
+                    }
+                    tmp[base + k * inner + in] = sum;
+                }
+            }
+        }
+        buf.swap(tmp);
+        inner = block;
+    }
+    for (long long i = 0; i < outer * xo; ++i) {
+        out[2 * i] = buf[i].real();
+        out[2 * i + 1] = buf[i].imag();
+    }
+    return 0;
+}
+
+const char* dfttest2_b200_version(void) {
+    return "dfttest2_b200 " DFTTEST2_B200_VERSION " (sm_100a; fused unit kernel, FP32 register codelets)";
+}
+
+const char* dfttest2_b200_last_error(void) { return g_last_error.c_str(); }
+
+}  // extern "C"

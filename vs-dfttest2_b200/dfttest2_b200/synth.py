@@ -1,0 +1,58 @@
+"""Seeded synthetic clips for tests and the benchmark.
+
+Clean content: 0.5 plus 16 drifting 2D sinusoids per plane,
+    0.5 + sum_k a_k sin(2 pi (fx_k (x - dx_k t) + fy_k (y - dy_k t)) + phi_k)
+with fx, fy ~ U[0, 0.25] cycles/px, a ~ U[0, 0.1], drift dx, dy ~ U[-1, 1]
+px/frame, phi ~ U[0, 2 pi).  Noise: additive i.i.d. Gaussian, optional
+salt-and-pepper.  Integer formats quantise round(clip(v, 0, 1) * peak).
+No public dataset is involved.
+
+The sum over sinusoids of each frame is one small matrix product
+(sin(a+b) = sin a cos b + cos a sin b), so full-HD clips build quickly.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .clip import FLOAT, Clip, VideoFormat, plane_dims
+
+
+def sinusoid_plane(rng: np.random.Generator, n: int, h: int, w: int, k: int = 16) -> np.ndarray:
+    fx = rng.uniform(0, 0.25, k)
+    fy = rng.uniform(0, 0.25, k)
+    a = rng.uniform(0, 0.1, k)
+    dx = rng.uniform(-1, 1, k)
+    dy = rng.uniform(-1, 1, k)
+    phi = rng.uniform(0, 2 * np.pi, k)
+    xs = np.arange(w, dtype=np.float64)
+    ys = np.arange(h, dtype=np.float64)
+    out = np.empty((n, h, w), np.float32)
+    for t in range(n):
+        ax = 2 * np.pi * np.outer(xs, fx)                              # (w, k)
+        ay = 2 * np.pi * np.outer(ys, fy) + (phi - 2 * np.pi * t * (fx * dx + fy * dy))  # (h, k)
+        left = np.concatenate([np.sin(ay) * a, np.cos(ay) * a], axis=1)   # (h, 2k)
+        right = np.concatenate([np.cos(ax), np.sin(ax)], axis=1).T        # (2k, w)
+        out[t] = (0.5 + left @ right).astype(np.float32)
+    return out
+
+
+def make_clip(fmt: VideoFormat, width: int, height: int, frames: int, seed: int, noise_sigma: float,
+              salt_pepper: float = 0.0) -> tuple[Clip, Clip]:
+    """Returns (noisy, clean) clips; noise_sigma is in [0, 1] units."""
+    rng = np.random.default_rng(seed)
+    noisy, clean = [], []
+    for p in range(fmt.num_planes):
+        pw, ph = plane_dims(fmt, width, height, p)
+        c = sinusoid_plane(rng, frames, ph, pw)
+        v = c + rng.standard_normal(c.shape, dtype=np.float32) * np.float32(noise_sigma)
+        if salt_pepper > 0:
+            u = rng.random(c.shape, dtype=np.float32)
+            v = np.where(u < salt_pepper / 2, 0.0, np.where(u < salt_pepper, 1.0, v)).astype(np.float32)
+        if fmt.sample_type == FLOAT:
+            noisy.append(v.astype(np.float32))
+            clean.append(c)
+        else:
+            peak = (1 << fmt.bits_per_sample) - 1
+            noisy.append(np.round(np.clip(v, 0, 1) * peak).astype(fmt.dtype))
+            clean.append(np.round(np.clip(c, 0, 1) * peak).astype(fmt.dtype))
+    return Clip(noisy, fmt), Clip(clean, fmt)
