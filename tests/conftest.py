@@ -24,6 +24,10 @@ def load_case(name):
     with open(os.path.join(GOLDEN, f"args_{name}.json")) as f:
         rec = json.load(f)
     args = dict(rec["args"])
+    # backend-specific options of the reference plugins (CPU ISA dispatch,
+    # cuFFT in-place, device selection) are not filter arguments
+    for k in ("opt", "in_place", "device_id", "num_streams"):
+        args.pop(k, None)
     args.setdefault("zero_mean", 1)
     args.setdefault("window_freq", None)
     args.setdefault("radius", 0)

@@ -16,6 +16,7 @@
 #include <complex>
 #include <condition_variable>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -50,7 +51,8 @@ int fail(int code, const std::string& msg) {
 using KernelFn = void (*)(const dft2::KernelArgs);
 
 struct Variant {
-    KernelFn main = nullptr;
+    KernelFn main = nullptr;      // Wiener fast path
+    KernelFn generic = nullptr;   // every filter type, asymmetric sigma
     KernelFn fixup = nullptr;
     int nw = 0;      // warps per CTA
     int bpw = 0;     // blocks per warp
@@ -60,7 +62,8 @@ struct Variant {
 template <int B, int T, int NW>
 Variant make_variant() {
     Variant v;
-    v.main = dft2::dfttest_unit_kernel<B, T, NW>;
+    v.main = dft2::dfttest_unit_kernel<B, T, NW, dft2::kFilterWiener>;
+    v.generic = dft2::dfttest_unit_kernel<B, T, NW, dft2::kFilterGeneric>;
     v.fixup = dft2::dfttest_fixup_kernel<B>;
     v.nw = NW;
     v.bpw = 64 / B;
@@ -69,8 +72,12 @@ Variant make_variant() {
 }
 
 // kernel variants per (block size, temporal size); NW keeps the per-warp
-// buffers plus rings within the shared-memory budget
+// buffers plus rings within the shared-memory budget.  DFTTEST2_B200_WARPS
+// selects an alternative CTA width where one is compiled.
 Variant select_variant(int B, int T) {
+    const char* env = std::getenv("DFTTEST2_B200_WARPS");
+    const int want = env ? std::atoi(env) : 0;
+    if (B == 16 && T == 3 && want == 4) return make_variant<16, 3, 4>();
     switch (B) {
 #ifndef DFTTEST2_B200_ONLY_B16
     case 8:
@@ -331,8 +338,9 @@ int launch(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, floa
     a.error_flag = slot.d_error;
 
     const size_t smem = f->var.smem(plan.pitch);
-    CUDA_TRY(cudaFuncSetAttribute(f->var.main, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    f->var.main<<<plan.nunits, f->var.nw * 32, smem, stream>>>(a);
+    KernelFn kern = (f->filter_type == 0 && !f->asym) ? f->var.main : f->var.generic;
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<plan.nunits, f->var.nw * 32, smem, stream>>>(a);
     CUDA_TRY(cudaGetLastError());
     if (plan.nfix > 0) {
         const int threads = 256;

@@ -130,10 +130,12 @@ __device__ __forceinline__ float load_sample(const void* base, long long idx, in
     return __ldg(reinterpret_cast<const float*>(base) + idx);
 }
 
-__device__ __forceinline__ void store_sample(void* base, long long idx, float acc, int kind, float scale, float peak) {
+__device__ __forceinline__ void store_sample(void* base, long long idx, float acc, int kind, float scale, float peak,
+                                             float inv_scale = 0.0f) {
     // cpu_source/getframe_impl.cpp:177-221: v = acc / scale, integers rounded
-    // by truncation of v + 0.5 and clamped to [0, peak]
-    const float v = __fdiv_rn(acc, scale);
+    // by truncation of v + 0.5 and clamped to [0, peak]; for the power-of-two
+    // integer scales the division is an exact multiplication (inv_scale)
+    const float v = inv_scale != 0.0f ? acc * inv_scale : __fdiv_rn(acc, scale);
     if (kind == kF32) {
         reinterpret_cast<float*>(base)[idx] = v;
         return;
@@ -148,11 +150,20 @@ __device__ __forceinline__ void store_sample(void* base, long long idx, float ac
         reinterpret_cast<uint16_t*>(base)[idx] = (uint16_t)q;
 }
 
-// multiplier of frequency_filtering (cpu_source/kernel.hpp:1826-1890)
+// reciprocal from the MUFU unit (PTX rcp.approx.ftz.f32, < 1 ulp)
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// multiplier of frequency_filtering (cpu_source/kernel.hpp:1826-1890).
+// FT 0 is the Wiener gain max((psd - s) / (psd + 1e-15), 0), evaluated as
+// max(1 - s * rcp(psd + 1e-15), 0); the other types keep IEEE division.
 template <int FT>
 __device__ __forceinline__ float gain(float psd, float s, const KernelArgs& a) {
     if constexpr (FT == 0) {
-        return fmaxf(__fdiv_rn(psd - s, psd + 1e-15f), 0.0f);
+        return fmaxf(fmaf(-s, rcp_approx(psd + 1e-15f), 1.0f), 0.0f);
     } else if constexpr (FT == 1) {
         return psd < s ? 0.0f : 1.0f;
     } else if constexpr (FT == 2) {
@@ -168,15 +179,38 @@ __device__ __forceinline__ float gain(float psd, float s, const KernelArgs& a) {
     }
 }
 
-// zero-mean gain of one bin: Y = m(|U - gW|^2) * (U - gW) + gW
-template <int FT>
-__device__ __forceinline__ void apply_bin(float& re, float& im, float s, float s2, bool dual, float wre, float wim,
-                                          float g, const KernelArgs& a) {
-    const float dre = fmaf(-g, wre, re);
-    const float dim = fmaf(-g, wim, im);
+__device__ __forceinline__ float gain_rt(int ft, float psd, float s, const KernelArgs& a) {
+    switch (ft) {
+    case 0: return fmaxf(__fdiv_rn(psd - s, psd + 1e-15f), 0.0f);
+    case 1: return gain<1>(psd, s, a);
+    case 2: return gain<2>(psd, s, a);
+    case 3: return gain<3>(psd, s, a);
+    case 4: return gain<4>(psd, s, a);
+    case 5: return gain<5>(psd, s, a);
+    default: return gain<6>(psd, s, a);
+    }
+}
+
+// kernel filter classes: the Wiener fast path, or every type with a runtime
+// switch (also handles asymmetric sigma on the packed columns)
+constexpr int kFilterWiener = 0;
+constexpr int kFilterGeneric = 7;
+
+// Y = m(|U - gW|^2) * (U - gW) + gW   (remove_mean / filter / add_mean,
+// cpu_source/kernel.hpp:1943-1952)
+template <int FC>
+__device__ __forceinline__ void apply_bin(float& re, float& im, float s, float s2, bool dual, float2 w, float g,
+                                          const KernelArgs& a) {
+    const float dre = fmaf(-g, w.x, re);
+    const float dim = fmaf(-g, w.y, im);
     const float psd = fmaf(dim, dim, dre * dre);
-    float m = gain<FT>(psd, s, a);
-    if (dual) m = 0.5f * (m + gain<FT>(psd, s2, a));
+    float m;
+    if constexpr (FC == kFilterWiener) {
+        m = gain<0>(psd, s, a);
+    } else {
+        m = gain_rt(a.filter_type, psd, s, a);
+        if (dual) m = 0.5f * (m + gain_rt(a.filter_type, psd, s2, a));
+    }
     re = fmaf(m, dre, re - dre);
     im = fmaf(m, dim, im - dim);
 }
@@ -205,7 +239,8 @@ struct Layout {
     static constexpr int o_sig = o_wsyn + B * WP;
     static constexpr int o_sig2 = o_sig + T * NSLOT * H;
     static constexpr int o_wfe = o_sig2 + T * NSLOT * H;
-    static constexpr int o_wbuf = o_wfe + 2 * T * NSLOT * H;
+    static constexpr int o_g = o_wfe + 2 * T * NSLOT * H;
+    static constexpr int o_wbuf = o_g + ((NW * BPW + 3) & ~3);
     static constexpr int o_ring = o_wbuf + NW * BPW * BSTR;
     __host__ __device__ static int in_ring_floats(int pitch) { return T * B * pitch; }
     __host__ __device__ static int ola_floats(int pitch) { return B * pitch; }
@@ -214,12 +249,17 @@ struct Layout {
     }
 };
 
+// i / n and i % n for small non-negative i, n through a float reciprocal
+// (exact while i * n < 2^22, which the shared-memory extents guarantee)
+__device__ __forceinline__ int div_small(int i, float inv_n) { return __float2int_rz(((float)i + 0.5f) * inv_n); }
+
 // ---------------------------------------------------------------------------
-// row phase: T rows of one block at one y -> packed spectra per temporal plane
+// row phase: T rows of one block at one y -> packed spectra per temporal plane;
+// returns this row's contribution to the block's 3D DC (zero-mean)
 // ---------------------------------------------------------------------------
 template <int B, int T>
-__device__ __forceinline__ void row_task(float* __restrict__ wb, const float* __restrict__ ring, int pitch, int slot_y,
-                                         int xoff, const float* __restrict__ win, int y, bool vec) {
+__device__ __forceinline__ float row_task(float* __restrict__ wb, const float* __restrict__ ring, int pitch, int slot_y,
+                                          int xoff, const float* __restrict__ win, int y, bool vec, bool store) {
     using TL = Tile<B>;
     constexpr int H = B / 2;
     constexpr int R = (T - 1) / 2;
@@ -289,15 +329,25 @@ __device__ __forceinline__ void row_task(float* __restrict__ wb, const float* __
             }
         }
     }
+    if (store) {
 #pragma unroll
-    for (int p = 0; p < T; ++p) {
-        float* dst = wb + p * B * B;
+        for (int p = 0; p < T; ++p) {
+            float* dst = wb + p * B * B;
 #pragma unroll
-        for (int q = 0; q < B / 4; ++q) {
-            *reinterpret_cast<float4*>(dst + TL::off(y, 4 * q)) =
-                make_float4(X[p][4 * q], X[p][4 * q + 1], X[p][4 * q + 2], X[p][4 * q + 3]);
+            for (int q = 0; q < B / 4; ++q) {
+                *reinterpret_cast<float4*>(dst + TL::off(y, 4 * q)) =
+                    make_float4(X[p][4 * q], X[p][4 * q + 1], X[p][4 * q + 2], X[p][4 * q + 3]);
+            }
         }
     }
+    return X[0][0];
+}
+
+// sum over the B lanes (rows) of one block; lanes of a block are contiguous
+template <int B> __device__ __forceinline__ float block_row_sum(float v) {
+#pragma unroll
+    for (int o = (B < 32 ? B : 32) / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
 }
 
 // ---------------------------------------------------------------------------
@@ -320,7 +370,7 @@ template <int B> __host__ __device__ constexpr int slot0_reg(int j) {
 }
 
 // gain of every bin of one plane held in (re, im); slot tables are [B+2][H]
-template <int B, int FT, bool PLANE0>
+template <int B, int FC, bool PLANE0>
 __device__ __forceinline__ void gain_plane(float (&re)[B], float (&im)[B], const float* __restrict__ sig,
                                            const float* __restrict__ sig2, const float* __restrict__ wfe, int c,
                                            float g, bool dual, const KernelArgs& a) {
@@ -329,43 +379,22 @@ __device__ __forceinline__ void gain_plane(float (&re)[B], float (&im)[B], const
     for (int j = 0; j < B; ++j) {
         const int r = PLANE0 ? slot0_reg<B>(j) : j;
         const float s = sig[j * H + c];
-        const float s2 = dual ? sig2[j * H + c] : s;
+        const float s2 = (FC != kFilterWiener && dual) ? sig2[j * H + c] : s;
         const float2 w = reinterpret_cast<const float2*>(wfe)[j * H + c];
-        apply_bin<FT>(re[r], im[r], s, s2, dual, w.x, w.y, g, a);
+        apply_bin<FC>(re[r], im[r], s, s2, dual, w, g, a);
     }
 }
 
-template <int B, int FT, bool PLANE0>
-__device__ __forceinline__ void gain_plane_dispatch(int ft, float (&re)[B], float (&im)[B], const float* sig,
-                                                    const float* sig2, const float* wfe, int c, float g, bool dual,
-                                                    const KernelArgs& a) {
-    switch (ft) {
-    case 0: gain_plane<B, 0, PLANE0>(re, im, sig, sig2, wfe, c, g, dual, a); break;
-    case 1: gain_plane<B, 1, PLANE0>(re, im, sig, sig2, wfe, c, g, dual, a); break;
-    case 2: gain_plane<B, 2, PLANE0>(re, im, sig, sig2, wfe, c, g, dual, a); break;
-    case 3: gain_plane<B, 3, PLANE0>(re, im, sig, sig2, wfe, c, g, dual, a); break;
-    case 4: gain_plane<B, 4, PLANE0>(re, im, sig, sig2, wfe, c, g, dual, a); break;
-    case 5: gain_plane<B, 5, PLANE0>(re, im, sig, sig2, wfe, c, g, dual, a); break;
-    default: gain_plane<B, 6, PLANE0>(re, im, sig, sig2, wfe, c, g, dual, a); break;
-    }
-}
-
-__device__ __forceinline__ void apply_bin_dispatch(int ft, float& re, float& im, float s, float s2, bool dual,
-                                                   float wre, float wim, float g, const KernelArgs& a) {
-    switch (ft) {
-    case 0: apply_bin<0>(re, im, s, s2, dual, wre, wim, g, a); break;
-    case 1: apply_bin<1>(re, im, s, s2, dual, wre, wim, g, a); break;
-    case 2: apply_bin<2>(re, im, s, s2, dual, wre, wim, g, a); break;
-    case 3: apply_bin<3>(re, im, s, s2, dual, wre, wim, g, a); break;
-    case 4: apply_bin<4>(re, im, s, s2, dual, wre, wim, g, a); break;
-    case 5: apply_bin<5>(re, im, s, s2, dual, wre, wim, g, a); break;
-    default: apply_bin<6>(re, im, s, s2, dual, wre, wim, g, a); break;
-    }
-}
-
-// one column task: lane (block, c) of a warp buffer block `wb`
-template <int B, int T>
-__device__ __forceinline__ void column_task(float* __restrict__ wb, const float* __restrict__ sm_sig,
+// one column task: lane (block, c) of a warp buffer block `wb`.
+//
+// Every temporal plane p is transformed along y, filtered, weighted by its
+// centre-frame twiddle w^(p r) and summed into S.  The packed lane (c = 0)
+// holds, for p <= r, the spectrum A_p of x-bin 0 and, for p > r, the
+// spectrum B_q (q = T - p) of x-bin B/2; each plane enters S through its
+// Hermitian part, the B planes multiplied by i, so that after plane 0 the
+// packed lane holds S_A + i S_B and one inverse y-DFT yields both columns.
+template <int B, int T, int FC>
+__device__ __forceinline__ void column_task(float* __restrict__ wb, float g, const float* __restrict__ sm_sig,
                                             const float* __restrict__ sm_sig2, const float* __restrict__ sm_wfe, int c,
                                             bool dual_tables, const KernelArgs& a) {
     using TL = Tile<B>;
@@ -375,23 +404,11 @@ __device__ __forceinline__ void column_task(float* __restrict__ wb, const float*
     const bool packed = (c == 0);
     const bool dual = dual_tables && packed;
 
-    // zero-mean offset g = DC / Re(WF[0]) (cpu_source/kernel.hpp:1943-1946)
-    float g = 0.0f;
-    if (a.g_div != 0.0f) {
-        float dc = 0.0f;
+    float sr[B], si[B];
 #pragma unroll
-        for (int y = 0; y < B; ++y) dc += wb[TL::off(y, 0)];
-        g = __fdiv_rn(dc, a.g_div);
-    }
-
-    float slr[B], sli[B], shr[B], shi[B];
-#pragma unroll
-    for (int k = 0; k < B; ++k) { slr[k] = sli[k] = shr[k] = shi[k] = 0.0f; }
-
+    for (int k = 0; k < B; ++k) sr[k] = si[k] = 0.0f;
     float qr[B], qi[B];
-    // temporal planes 1..T-1: gain, then accumulate w^(p*r) * Y into the
-    // low (p <= r) or high half; the packed lane holds conj pairs in the
-    // high half, hence the conjugated twiddle there.
+
 #pragma unroll
     for (int p = 1; p < T; ++p) {
         const float* src = wb + p * B * B;
@@ -402,22 +419,40 @@ __device__ __forceinline__ void column_task(float* __restrict__ wb, const float*
             qi[y] = v.y;
         }
         ydft_fwd<B>(qr, qi);
-        gain_plane_dispatch<B, 0, false>(a.filter_type, qr, qi, sm_sig + p * NSLOT * H, sm_sig2 + p * NSLOT * H,
-                                         sm_wfe + 2 * p * NSLOT * H, c, g, dual, a);
-        const float twr = CentreTwiddle<T>::re(p);
-        const float twi = (packed && p > R) ? -CentreTwiddle<T>::im(p) : CentreTwiddle<T>::im(p);
-        if (p <= R) {
+        gain_plane<B, FC, false>(qr, qi, sm_sig + p * NSLOT * H, sm_sig2 + p * NSLOT * H, sm_wfe + 2 * p * NSLOT * H,
+                                 c, g, dual, a);
+        // twiddle: w^(p r) = (tc, ts); packed lane on a B plane uses i * conj(w^(p r))
+        const float tc = CentreTwiddle<T>::re(p), ts = CentreTwiddle<T>::im(p);
+        const bool swap = packed && (p > R);
+        const float twr = swap ? ts : tc;
+        const float twi = swap ? tc : ts;
 #pragma unroll
-            for (int k = 0; k < B; ++k) {
-                slr[k] = fmaf(qr[k], twr, fmaf(-qi[k], twi, slr[k]));
-                sli[k] = fmaf(qr[k], twi, fmaf(qi[k], twr, sli[k]));
-            }
-        } else {
+        for (int k = 0; k < B; ++k) {
+            const float vr = fmaf(qr[k], twr, -qi[k] * twi);
+            const float vi = fmaf(qr[k], twi, qi[k] * twr);
+            qr[k] = vr;
+            qi[k] = vi;
+        }
+        if (packed) {
+            // Hermitian part (A planes) or anti-Hermitian part (i * B planes)
+            const float sg = (p <= R) ? 1.0f : -1.0f;
+            qr[0] = qr[0] + sg * qr[0];
+            qi[0] = qi[0] - sg * qi[0];
+            qr[H] = qr[H] + sg * qr[H];
+            qi[H] = qi[H] - sg * qi[H];
 #pragma unroll
-            for (int k = 0; k < B; ++k) {
-                shr[k] = fmaf(qr[k], twr, fmaf(-qi[k], twi, shr[k]));
-                shi[k] = fmaf(qr[k], twi, fmaf(qi[k], twr, shi[k]));
+            for (int k = 1; k < H; ++k) {
+                const float ar = qr[k], ai = qi[k], br = qr[B - k], bi = qi[B - k];
+                qr[k] = fmaf(sg, br, ar);
+                qi[k] = fmaf(-sg, bi, ai);
+                qr[B - k] = fmaf(sg, ar, br);
+                qi[B - k] = fmaf(-sg, ai, bi);
             }
+        }
+#pragma unroll
+        for (int k = 0; k < B; ++k) {
+            sr[k] += qr[k];
+            si[k] += qi[k];
         }
     }
 
@@ -446,47 +481,35 @@ __device__ __forceinline__ void column_task(float* __restrict__ wb, const float*
         qi[H] = 0.0f;
         qi[0] = 0.0f;
     }
-    const float* sig0 = sm_sig;
-    const float* sig20 = sm_sig2;
-    const float* wfe0 = sm_wfe;
-    gain_plane_dispatch<B, 0, true>(a.filter_type, qr, qi, sig0, sig20, wfe0, c, g, dual, a);
+    gain_plane<B, FC, true>(qr, qi, sm_sig, sm_sig2, sm_wfe, c, g, dual, a);
     if (packed) {
-        const float2 w1 = reinterpret_cast<const float2*>(wfe0)[B * H + c];
-        const float2 w2 = reinterpret_cast<const float2*>(wfe0)[(B + 1) * H + c];
-        apply_bin_dispatch(a.filter_type, e1r, e1i, sig0[B * H + c], dual ? sig20[B * H + c] : 0.0f, dual, w1.x, w1.y,
-                           g, a);
-        apply_bin_dispatch(a.filter_type, e2r, e2i, sig0[(B + 1) * H + c], dual ? sig20[(B + 1) * H + c] : 0.0f, dual,
-                           w2.x, w2.y, g, a);
-        // Hermitian sums S_A = Y_A0 + L + conj(L(-k)), S_B likewise, Z = S_A + i S_B
+        const float2 w1 = reinterpret_cast<const float2*>(sm_wfe)[B * H + c];
+        const float2 w2 = reinterpret_cast<const float2*>(sm_wfe)[(B + 1) * H + c];
+        apply_bin<FC>(e1r, e1i, sm_sig[B * H + c], dual ? sm_sig2[B * H + c] : 0.0f, dual, w1, g, a);
+        apply_bin<FC>(e2r, e2i, sm_sig[(B + 1) * H + c], dual ? sm_sig2[(B + 1) * H + c] : 0.0f, dual, w2, g, a);
+        // add Y_A0 + i Y_B0, both Hermitian in y
+        sr[0] += qr[0];
+        si[0] += qr[H];
+        sr[H] += e1r;
+        si[H] += e2r;
 #pragma unroll
         for (int k = 1; k < H; ++k) {
-            const float sar = qr[k] + slr[k] + slr[B - k];
-            const float sai = qi[k] + sli[k] - sli[B - k];
-            const float sbr = qr[B - k] + shr[k] + shr[B - k];
-            const float sbi = qi[B - k] + shi[k] - shi[B - k];
-            qr[k] = sar - sbi;
-            qi[k] = sai + sbr;
-            qr[B - k] = sar + sbi;
-            qi[B - k] = sbr - sai;
+            const float ar = qr[k], ai = qi[k], br = qr[B - k], bi = qi[B - k];
+            sr[k] += ar - bi;
+            si[k] += ai + br;
+            sr[B - k] += ar + bi;
+            si[B - k] += br - ai;
         }
-        const float sa0 = fmaf(2.0f, slr[0], qr[0]);
-        const float sb0 = fmaf(2.0f, shr[0], qr[H]);
-        const float sah = fmaf(2.0f, slr[H], e1r);
-        const float sbh = fmaf(2.0f, shr[H], e2r);
-        qr[0] = sa0;
-        qi[0] = sb0;
-        qr[H] = sah;
-        qi[H] = sbh;
     } else {
 #pragma unroll
         for (int k = 0; k < B; ++k) {
-            qr[k] += slr[k] + shr[k];
-            qi[k] += sli[k] + shi[k];
+            sr[k] += qr[k];
+            si[k] += qi[k];
         }
     }
-    ydft_inv<B>(qr, qi);
+    ydft_inv<B>(sr, si);
 #pragma unroll
-    for (int y = 0; y < B; ++y) *reinterpret_cast<float2*>(wb + TL::off(y, 2 * c)) = make_float2(qr[y], qi[y]);
+    for (int y = 0; y < B; ++y) *reinterpret_cast<float2*>(wb + TL::off(y, 2 * c)) = make_float2(sr[y], si[y]);
 }
 
 // inverse rows: packed row -> real, synthesis window, in place
@@ -514,11 +537,13 @@ __device__ __forceinline__ void inverse_row_task(float* __restrict__ wb, const f
     }
 }
 
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // ---------------------------------------------------------------------------
 // main kernel
 // ---------------------------------------------------------------------------
-template <int B, int T, int NW>
-__global__ void __launch_bounds__(NW * 32, 1) dfttest_unit_kernel(const __grid_constant__ KernelArgs a) {
+template <int B, int T, int NW, int FC>
+__global__ void __launch_bounds__(NW * 32, NW <= 4 ? 2 : 1) dfttest_unit_kernel(const __grid_constant__ KernelArgs a) {
     using L = Layout<B, T, NW>;
     using TL = Tile<B>;
     constexpr int H = B / 2;
@@ -555,6 +580,8 @@ __global__ void __launch_bounds__(NW * 32, 1) dfttest_unit_kernel(const __grid_c
         return;
     }
     float* rec = a.scratch + (size_t)uid * a.rec_stride;
+    const bool is_float = (a.kind == kF32);
+    const float inv_scale = 1.0f / a.scale;  // exact for the power-of-two integer scales
 
     // --- constants into shared memory -----------------------------------
     float* s_win = sm + L::o_win;
@@ -562,23 +589,25 @@ __global__ void __launch_bounds__(NW * 32, 1) dfttest_unit_kernel(const __grid_c
     float* s_sig = sm + L::o_sig;
     float* s_sig2 = sm + L::o_sig2;
     float* s_wfe = sm + L::o_wfe;
+    float* s_g = sm + L::o_g;
     float* s_wbuf = sm + L::o_wbuf;
     float* s_in = sm + L::o_ring;
     float* s_ola = s_in + L::in_ring_floats(pitch);
     // scale * window, rounded once as in load_block (cpu_source/getframe_impl.cpp:137)
     for (int i = tid; i < T * B * B; i += NT) s_win[(i / B) * TL::WP + (i % B)] = a.scale * a.win[i];
     for (int i = tid; i < B * B; i += NT) s_wsyn[(i / B) * TL::WP + (i % B)] = a.wsyn[i];
+    const bool dual_tables = (FC != kFilterWiener) && a.sig2 != nullptr;
     for (int i = tid; i < T * L::NSLOT * H; i += NT) {
         s_sig[i] = a.sig[i];
-        s_sig2[i] = a.sig2 ? a.sig2[i] : a.sig[i];
+        if (dual_tables) s_sig2[i] = a.sig2[i];
     }
     for (int i = tid; i < 2 * T * L::NSLOT * H; i += NT) s_wfe[i] = a.wfe[i];
     for (int i = tid; i < L::ola_floats(pitch); i += NT) s_ola[i] = 0.0f;
-    const bool dual_tables = a.sig2 != nullptr;
 
     const int fw = u.fw;
     const int x0 = u.bx0 * S;  // footprint origin (padded coordinates)
     const bool vec = ((S & 3) == 0);
+    const float inv_fw = 1.0f / (float)fw;
 
     for (int by = u.by0; by <= u.by1; ++by) {
         // ---- finalize rows of the previous step + stage input rows of this one
@@ -586,18 +615,21 @@ __global__ void __launch_bounds__(NW * 32, 1) dfttest_unit_kernel(const __grid_c
             const int pb = by - 1;
             const bool last = (pb == u.by1 - 1);
             const int nrows = last ? B : S;
+            const int excl_y0 = u.by0 * S + O, excl_y1 = u.by1 * S;
+            const int excl_x0 = x0 + O, excl_x1 = u.bx1 * S;
             for (int i = tid; i < nrows * fw; i += NT) {
-                const int r = i / fw, lx = i % fw;
+                const int r = div_small(i, inv_fw);
+                const int lx = i - r * fw;
                 const int py = pb * S + r;
                 float* cell = s_ola + (py % B) * pitch + lx;
                 const float v = *cell;
                 *cell = 0.0f;
                 const int px = x0 + lx;
                 if (px < ox || px >= ox + W || py < oy || py >= oy + Hh) continue;
-                const bool excl = (px >= x0 + O) && (px < u.bx1 * S) && (py >= u.by0 * S + O) && (py < u.by1 * S);
+                const bool excl = (px >= excl_x0) && (px < excl_x1) && (py >= excl_y0) && (py < excl_y1);
                 if (excl) {
                     store_sample(job.dst, (long long)(py - oy) * job.dst_stride + (px - ox), v, a.kind, a.scale,
-                                 a.peak);
+                                 a.peak, is_float ? 0.0f : inv_scale);
                 } else {
                     rec[band_index(lx, py - u.by0 * S, fw, u.fh, O)] = v;
                 }
@@ -609,15 +641,32 @@ __global__ void __launch_bounds__(NW * 32, 1) dfttest_unit_kernel(const __grid_c
             const int r_hi = by * S + B;
             const int nr = r_hi - r_lo;
             const int rowlen = nbx * S + O;  // footprint width of this step
-            for (int i = tid; i < T * nr * rowlen; i += NT) {
-                const int t = i / (nr * rowlen);
-                const int rem = i - t * nr * rowlen;
-                const int r = rem / rowlen, lx = rem - r * rowlen;
-                const int py = r_lo + r;
-                const int sy_ = mirror(py - oy, Hh);
-                const int sx_ = mirror(x0 + lx - ox, W);
-                s_in[(t * B + (py % B)) * pitch + lx] =
-                    load_sample(job.src[t], (long long)sy_ * job.src_stride + sx_, a.kind);
+            for (int row = warp; row < T * nr; row += NW) {
+                const int t = row / nr;
+                const int py = r_lo + (row - t * nr);
+                const long long sy_ = mirror(py - oy, Hh);
+                const void* base = job.src[t];
+                for (int lx = lane; lx < rowlen; lx += 32) {
+                    const int sx_ = mirror(x0 + lx - ox, W);
+                    s_in[(t * B + (py % B)) * pitch + lx] = load_sample(base, sy_ * job.src_stride + sx_, a.kind);
+                }
+            }
+            // warm L2 with the rows of the next step (one request per 128 B)
+            if (by + 1 < u.by1) {
+                const int npy = r_hi;  // first new row of the next step
+                const int esz = a.kind == kF32 ? 4 : (a.kind == kU16 ? 2 : 1);
+                const int sx_lo = max(x0 - ox, 0), sx_hi = max(min(x0 + rowlen - ox, W) - 1, sx_lo);
+                const int nline = (int)(((long long)(sx_hi - sx_lo) * esz) / 128) + 2;
+                for (int i = tid; i < T * S * nline; i += NT) {
+                    const int t = i / (S * nline);
+                    const int rem = i - t * S * nline;
+                    const int r = rem / nline, li = rem - r * nline;
+                    const int py = npy + r;
+                    if (py >= ph) continue;
+                    const long long sy_ = mirror(py - oy, Hh);
+                    const int sxp = min(sx_lo + li * (128 / esz), sx_hi);
+                    prefetch_l2(reinterpret_cast<const char*>(job.src[t]) + (sy_ * job.src_stride + sxp) * esz);
+                }
             }
         }
         __syncthreads();
@@ -625,21 +674,28 @@ __global__ void __launch_bounds__(NW * 32, 1) dfttest_unit_kernel(const __grid_c
         // ---- per-warp block transforms
         {
             float* wb0 = s_wbuf + warp * BPW * L::BSTR;
-            // row phase: 2 tasks per lane
+            // row phase: 2 tasks per lane; the DC of each block is summed
+            // over its rows with shuffles (lanes of a block are contiguous)
 #pragma unroll
             for (int k = 0; k < 2; ++k) {
                 const int gr = k * 32 + lane;
                 const int b = gr / B, y = gr % B;
                 const int bl = warp * BPW + b;
-                if (bl < nbx) {
-                    row_task<B, T>(wb0 + b * L::BSTR, s_in, pitch, (by * S + y) % B, bl * S, s_win, y, vec);
-                }
+                const bool valid = bl < nbx;
+                const int blr = valid ? bl : nbx - 1;
+                const float dc = row_task<B, T>(wb0 + b * L::BSTR, s_in, pitch, (by * S + y) % B, blr * S, s_win, y,
+                                                vec, valid);
+                const float tot = block_row_sum<B>(dc);
+                // g = DC / Re(WF[0]) (cpu_source/kernel.hpp:1945)
+                if (y == 0 && valid) s_g[warp * BPW + b] = a.g_div != 0.0f ? __fdiv_rn(tot, a.g_div) : 0.0f;
             }
             __syncwarp();
             {
                 const int b = lane / H, c = lane % H;
                 const int bl = warp * BPW + b;
-                if (bl < nbx) column_task<B, T>(wb0 + b * L::BSTR, s_sig, s_sig2, s_wfe, c, dual_tables, a);
+                if (bl < nbx)
+                    column_task<B, T, FC>(wb0 + b * L::BSTR, s_g[warp * BPW + b], s_sig, s_sig2, s_wfe, c, dual_tables,
+                                          a);
             }
             __syncwarp();
 #pragma unroll
@@ -657,8 +713,9 @@ __global__ void __launch_bounds__(NW * 32, 1) dfttest_unit_kernel(const __grid_c
             const int rowlen = nbx * S + O;
             if (vec) {
                 const int nq = rowlen >> 2;
+                const float inv_nq = 1.0f / (float)nq;
                 for (int i = tid; i < B * nq; i += NT) {
-                    const int r = i / nq, q = i - r * nq;
+                    const int r = div_small(i, inv_nq), q = i - r * nq;
                     const int px = 4 * q;
                     int b_lo = px - B + 4;
                     b_lo = b_lo <= 0 ? 0 : (b_lo + S - 1) / S;
@@ -666,7 +723,7 @@ __global__ void __launch_bounds__(NW * 32, 1) dfttest_unit_kernel(const __grid_c
                     b_hi = b_hi < nbx - 1 ? b_hi : nbx - 1;
                     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
                     for (int bl = b_lo; bl <= b_hi; ++bl) {
-                        const float* ob = s_wbuf + (bl / BPW) * BPW * L::BSTR + (bl % BPW) * L::BSTR;
+                        const float* ob = s_wbuf + bl * L::BSTR;
                         const float4 v = *reinterpret_cast<const float4*>(ob + TL::off(r, px - bl * S));
                         acc.x += v.x;
                         acc.y += v.y;
@@ -682,17 +739,15 @@ __global__ void __launch_bounds__(NW * 32, 1) dfttest_unit_kernel(const __grid_c
                     *cell = c4;
                 }
             } else {
+                const float inv_rl = 1.0f / (float)rowlen;
                 for (int i = tid; i < B * rowlen; i += NT) {
-                    const int r = i / rowlen, px = i - r * rowlen;
+                    const int r = div_small(i, inv_rl), px = i - r * rowlen;
                     int b_lo = px - B + 1;
                     b_lo = b_lo <= 0 ? 0 : (b_lo + S - 1) / S;
                     int b_hi = px / S;
                     b_hi = b_hi < nbx - 1 ? b_hi : nbx - 1;
                     float acc = 0.0f;
-                    for (int bl = b_lo; bl <= b_hi; ++bl) {
-                        const float* ob = s_wbuf + (bl / BPW) * BPW * L::BSTR + (bl % BPW) * L::BSTR;
-                        acc += ob[TL::off(r, px - bl * S)];
-                    }
+                    for (int bl = b_lo; bl <= b_hi; ++bl) acc += s_wbuf[bl * L::BSTR + TL::off(r, px - bl * S)];
                     s_ola[((by * S + r) % B) * pitch + px] += acc;
                 }
             }
