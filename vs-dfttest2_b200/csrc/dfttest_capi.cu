@@ -59,50 +59,50 @@ struct Variant {
     size_t (*smem)(int pitch) = nullptr;
 };
 
-template <int B, int T, int NW>
+template <int B, int T, int NW, int MINB = 1>
 Variant make_variant() {
     Variant v;
-    v.main = dft2::dfttest_unit_kernel<B, T, NW, dft2::kFilterWiener>;
-    v.generic = dft2::dfttest_unit_kernel<B, T, NW, dft2::kFilterGeneric>;
+    v.main = dft2::dfttest_unit_kernel<B, T, NW, dft2::kFilterWiener, MINB>;
+    v.generic = dft2::dfttest_unit_kernel<B, T, NW, dft2::kFilterGeneric, MINB>;
     v.fixup = dft2::dfttest_fixup_kernel<B>;
     v.nw = NW;
-    v.bpw = 64 / B;
+    v.bpw = 32 / B;
     v.smem = [](int pitch) { return dft2::Layout<B, T, NW>::smem_bytes(pitch); };
     return v;
 }
 
-// kernel variants per (block size, temporal size); NW keeps the per-warp
-// buffers plus rings within the shared-memory budget.  DFTTEST2_B200_WARPS
-// selects an alternative CTA width where one is compiled.
+// kernel variants per (block size, temporal size): NW warps per CTA keeps
+// the per-warp block buffers plus the rings within 227 KB of shared memory
+// (and 16 warps cap registers at 128 per thread)
 Variant select_variant(int B, int T) {
+    // DFTTEST2_B200_WARPS=16 selects the one-CTA-per-SM shape for 16x16x3
     const char* env = std::getenv("DFTTEST2_B200_WARPS");
-    const int want = env ? std::atoi(env) : 0;
-    if (B == 16 && T == 3 && want == 4) return make_variant<16, 3, 4>();
+    if (env && B == 16 && T == 3 && std::atoi(env) == 16) return make_variant<16, 3, 16>();
     switch (B) {
 #ifndef DFTTEST2_B200_ONLY_B16
     case 8:
         switch (T) {
-        case 1: return make_variant<8, 1, 8>();
-        case 3: return make_variant<8, 3, 8>();
-        case 5: return make_variant<8, 5, 8>();
-        case 7: return make_variant<8, 7, 8>();
+        case 1: return make_variant<8, 1, 16>();
+        case 3: return make_variant<8, 3, 16>();
+        case 5: return make_variant<8, 5, 16>();
+        case 7: return make_variant<8, 7, 16>();
         }
         break;
 #endif
     case 16:
         switch (T) {
-        case 1: return make_variant<16, 1, 8>();
-        case 3: return make_variant<16, 3, 8>();
-        case 5: return make_variant<16, 5, 4>();
-        case 7: return make_variant<16, 7, 4>();
+        case 1: return make_variant<16, 1, 16>();
+        case 3: return make_variant<16, 3, 8, 2>();
+        case 5: return make_variant<16, 5, 12>();
+        case 7: return make_variant<16, 7, 8>();
         }
         break;
 #ifndef DFTTEST2_B200_ONLY_B16
     case 32:
         switch (T) {
-        case 1: return make_variant<32, 1, 8>();
-        case 3: return make_variant<32, 3, 4>();
-        case 5: return make_variant<32, 5, 2>();
+        case 1: return make_variant<32, 1, 16>();
+        case 3: return make_variant<32, 3, 8>();
+        case 5: return make_variant<32, 5, 4>();
         case 7: return make_variant<32, 7, 2>();
         }
         break;
@@ -145,6 +145,7 @@ struct dfttest2_b200_filter {
     float* d_sig = nullptr;
     float* d_sig2 = nullptr;
     float* d_wfe = nullptr;
+    int wmask = 0;
 
     std::vector<Slot> slots;
     std::vector<int> free_slots;
@@ -332,6 +333,7 @@ int launch(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, floa
     a.sig = f->d_sig;
     a.sig2 = f->asym ? f->d_sig2 : nullptr;
     a.wfe = f->d_wfe;
+    a.wmask = f->zero_mean ? f->wmask : 0;
     a.scratch = slot.d_scratch;
     a.rec_stride = plan.rec_stride;
     a.ring_pitch = plan.pitch;
@@ -470,52 +472,63 @@ int dfttest2_b200_create(const dfttest2_b200_params* p, dfttest2_b200_filter** o
         if (!zero_mean) return 0.0f;
         return (float)p->window_freq[((t * B + y) * X + x) * 2 + part];
     };
-    const int NS = B + 2;
-    std::vector<float> sig(T * NS * H), sig2(T * NS * H), wfe(2 * T * NS * H);
+    // Gain-slot tables, laid out [plane][slot][lane w = 2c + h] as the column
+    // phase reads them: lane (c, h) holds the y-bins k = 2m + h of packed
+    // x-column c; column 0 carries x-bins 0 (A) and B/2 (B).  sig2 is the
+    // sigma of the Hermitian partner bin (t, -k) of packed-column bins.
+    const int M = B / 2, NS = M + 2;
+    std::vector<float> sig(T * NS * B), sig2(T * NS * B), wfe(2 * T * NS * B);
     bool asym = false;
-    // gain slot j of plane p for lane column c -> spectrum bin (t, y, x) and
-    // the Hermitian partner bin of the packed columns
-    auto put = [&](int pl, int j, int c, int t, int y, int x, int t2, int y2) {
-        const int idx = (pl * NS + j) * H + c;
+    auto put = [&](int pl, int j, int w, int t, int y, int x, int t2, int y2) {
+        const int idx = (pl * NS + j) * B + w;
         sig[idx] = sigma_at(t, y, x);
         sig2[idx] = sigma_at(t2, y2, x);
         wfe[2 * idx] = wf_at(t, y, x, 0);
         wfe[2 * idx + 1] = wf_at(t, y, x, 1);
         if (sig2[idx] != sig[idx]) asym = true;
     };
+    auto neg = [&](int k) { return (B - k) % B; };
     for (int pl = 0; pl < T; ++pl) {
-        for (int c = 0; c < H; ++c) {
-            if (pl == 0) {
-                for (int j = 0; j < B; ++j) {
-                    const int k = j >> 1;
-                    if (c > 0) {
-                        const int y = j == 0 ? 0 : (j == 1 ? H : ((j & 1) ? B - k : k));
-                        put(0, j, c, 0, y, c, 0, y);
-                    } else {
-                        // packed plane 0: A (x=0) at even slots, B (x=H) at odd slots
-                        const int ky = (j < 2) ? 0 : k;
-                        const int x = (j & 1) ? H : 0;
-                        put(0, j, 0, 0, ky, x, 0, (B - ky) % B);
-                    }
+        for (int w = 0; w < B; ++w) {
+            const int c = w >> 1, h = w & 1;
+            for (int j = 0; j < NS; ++j) put(pl, j, w, 0, 0, 0, 0, 0);  // unused slots
+            if (c > 0) {
+                for (int m = 0; m < M; ++m) put(pl, m, w, pl, 2 * m + h, c, pl, 2 * m + h);
+                continue;
+            }
+            if (pl > 0) {
+                for (int m = 0; m < M; ++m) {
+                    const int k = 2 * m + h;
+                    if (pl <= radius) put(pl, m, w, pl, k, 0, T - pl, neg(k));
+                    else put(pl, m, w, T - pl, k, H, pl, neg(k));
                 }
-                // extra packed slots: Nyquist-y bins of columns 0 and H
-                put(0, B, c, 0, H, 0, 0, H);
-                put(0, B + 1, c, 0, H, H, 0, H);
+                continue;
+            }
+            // plane 0 of the packed column: untangled A (x-bin 0) and B (x-bin B/2)
+            if (h == 0) {
+                put(0, 0, w, 0, 0, 0, 0, 0);            // A(0)
+                put(0, M / 2, w, 0, H, 0, 0, H);        // A(B/2)
+                for (int m = 1; m < M / 2; ++m) {
+                    put(0, m, w, 0, 2 * m, 0, 0, neg(2 * m));      // A(2m)
+                    put(0, M - m, w, 0, 2 * m, H, 0, neg(2 * m));  // B(2m)
+                }
+                put(0, M, w, 0, 0, H, 0, 0);            // B(0)
+                put(0, M + 1, w, 0, H, H, 0, H);        // B(B/2)
             } else {
-                for (int y = 0; y < B; ++y) {
-                    if (c > 0) {
-                        put(pl, y, c, pl, y, c, pl, y);
-                    } else if (pl <= radius) {
-                        put(pl, y, 0, pl, y, 0, T - pl, (B - y) % B);
-                    } else {
-                        put(pl, y, 0, T - pl, y, H, pl, (B - y) % B);
-                    }
+                for (int m = 0; m < M / 2; ++m) {
+                    put(0, m, w, 0, 2 * m + 1, 0, 0, neg(2 * m + 1));          // A(2m+1)
+                    put(0, M - 1 - m, w, 0, 2 * m + 1, H, 0, neg(2 * m + 1));  // B(2m+1)
                 }
-                put(pl, B, c, 0, 0, 0, 0, 0);
-                put(pl, B + 1, c, 0, 0, 0, 0, 0);
             }
         }
     }
+    // temporal planes whose window spectrum is identically zero skip the
+    // zero-mean terms (every plane but 0 for a rectangular temporal window)
+    int wmask = 0;
+    for (int pl = 0; pl < T; ++pl)
+        for (int i = 0; i < NS * B * 2; ++i)
+            if (wfe[pl * NS * B * 2 + i] != 0.0f) wmask |= 1 << pl;
+    f->wmask = wmask;
     f->asym = asym;
     f->g_div = zero_mean ? (float)p->window_freq[0] : 0.0f;
     if (zero_mean && f->g_div == 0.0f) return fail(DFTTEST2_B200_EINVAL, "window_freq[0] must be non-zero");

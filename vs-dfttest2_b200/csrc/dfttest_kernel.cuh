@@ -72,9 +72,10 @@ struct KernelArgs {
     float g_div;       // Re(window_freq[0,0,0]); 0 disables zero-mean
     const float* win;  // [T][B][B] analysis window * scale
     const float* wsyn; // [B][B] synthesis window
-    const float* sig;  // [T][B+2][B/2] sigma per gain slot
-    const float* sig2; // [T][B+2][B/2] partner sigma (packed lane, asymmetric sigma), may be null
-    const float* wfe;  // [T][B+2][B/2][2] window spectrum per gain slot (zero-mean)
+    const float* sig;  // [T][B/2+2][B] sigma per gain slot and column lane
+    const float* sig2; // [T][B/2+2][B] partner sigma (packed lanes, asymmetric sigma), may be null
+    const float* wfe;  // [T][B/2+2][B][2] window spectrum per gain slot (zero-mean)
+    int wmask;         // bit p set when temporal plane p of the window spectrum is not identically zero
     float* scratch;    // per-unit band records
     int rec_stride;    // floats per unit record
     int ring_pitch;    // floats per ring row
@@ -122,6 +123,18 @@ __device__ __forceinline__ int mirror(int i, int n) {
     // reflection without edge repeat (cpu_source/getframe_impl.cpp:44-62)
     i = i < 0 ? -i : i;
     return i >= n ? 2 * (n - 1) - i : i;
+}
+
+// raw sample bits (integer value or float bits); converting later keeps the
+// load in flight instead of stalling on it
+__device__ __forceinline__ unsigned load_raw(const void* base, long long idx, int kind) {
+    if (kind == kU8) return __ldg(reinterpret_cast<const uint8_t*>(base) + idx);
+    if (kind == kU16) return __ldg(reinterpret_cast<const uint16_t*>(base) + idx);
+    return __float_as_uint(__ldg(reinterpret_cast<const float*>(base) + idx));
+}
+
+__device__ __forceinline__ float raw_to_float(unsigned v, int kind) {
+    return kind == kF32 ? __uint_as_float(v) : (float)v;
 }
 
 __device__ __forceinline__ float load_sample(const void* base, long long idx, int kind) {
@@ -198,11 +211,12 @@ constexpr int kFilterGeneric = 7;
 
 // Y = m(|U - gW|^2) * (U - gW) + gW   (remove_mean / filter / add_mean,
 // cpu_source/kernel.hpp:1943-1952)
-template <int FC>
+// ZM = false: the plane's window spectrum is zero, so the zero-mean terms vanish
+template <int FC, bool ZM = true>
 __device__ __forceinline__ void apply_bin(float& re, float& im, float s, float s2, bool dual, float2 w, float g,
                                           const KernelArgs& a) {
-    const float dre = fmaf(-g, w.x, re);
-    const float dim = fmaf(-g, w.y, im);
+    const float dre = ZM ? fmaf(-g, w.x, re) : re;
+    const float dim = ZM ? fmaf(-g, w.y, im) : im;
     const float psd = fmaf(dim, dim, dre * dre);
     float m;
     if constexpr (FC == kFilterWiener) {
@@ -211,16 +225,23 @@ __device__ __forceinline__ void apply_bin(float& re, float& im, float s, float s
         m = gain_rt(a.filter_type, psd, s, a);
         if (dual) m = 0.5f * (m + gain_rt(a.filter_type, psd, s2, a));
     }
-    re = fmaf(m, dre, re - dre);
-    im = fmaf(m, dim, im - dim);
+    if constexpr (ZM) {
+        re = fmaf(m, dre, re - dre);
+        im = fmaf(m, dim, im - dim);
+    } else {
+        re *= m;
+        im *= m;
+    }
 }
 
 template <int B> struct Tile {
-    static constexpr int H = B / 2;          // packed x-bins per block (lanes per block)
-    static constexpr int BPW = 64 / B;       // blocks per warp
+    static constexpr int H = B / 2;          // packed x-bins per block
+    static constexpr int M = B / 2;          // y-bins per column lane (lane pair splits by parity)
+    static constexpr int BPW = 32 / B;       // blocks per warp (B lanes per block)
     static constexpr int WP = B + 4;         // padded window row pitch (floats)
     static constexpr int RPL = 32 / B;       // rows per 128-byte line in the warp buffer
     static constexpr int NCH = B / 4;        // 16-byte chunks per buffer row
+    static constexpr int NSLOT = M + 2;      // gain slots per lane and plane
     __device__ static __forceinline__ int swz(int y) { return (y / RPL) & (NCH - 1); }
     // float offset of (y, x) inside one B x B plane of the warp buffer
     __device__ static __forceinline__ int off(int y, int x) { return y * B + ((((x >> 2) ^ swz(y)) << 2) | (x & 3)); }
@@ -228,18 +249,21 @@ template <int B> struct Tile {
 
 template <int B, int T, int NW>
 struct Layout {
-    static constexpr int H = B / 2;
-    static constexpr int BPW = 64 / B;
+    static constexpr int M = B / 2;
+    static constexpr int BPW = 32 / B;
     static constexpr int WP = B + 4;
-    static constexpr int NSLOT = B + 2;
-    static constexpr int BSTR = T * B * B + B;  // warp-buffer floats per block
+    static constexpr int NSLOT = M + 2;
+    // warp-buffer floats per block; the stride is 4 (mod 32) floats so that the
+    // overlap-add, whose lanes read the same 16-byte chunk of consecutive
+    // blocks, spreads over 8 bank groups
+    static constexpr int BSTR = T * B * B + 4;
     // offsets in floats (ring sizes depend on the runtime pitch)
     static constexpr int o_win = 0;
     static constexpr int o_wsyn = o_win + T * B * WP;
     static constexpr int o_sig = o_wsyn + B * WP;
-    static constexpr int o_sig2 = o_sig + T * NSLOT * H;
-    static constexpr int o_wfe = o_sig2 + T * NSLOT * H;
-    static constexpr int o_g = o_wfe + 2 * T * NSLOT * H;
+    static constexpr int o_sig2 = o_sig + T * NSLOT * B;
+    static constexpr int o_wfe = o_sig2 + T * NSLOT * B;
+    static constexpr int o_g = o_wfe + 2 * T * NSLOT * B;
     static constexpr int o_wbuf = o_g + ((NW * BPW + 3) & ~3);
     static constexpr int o_ring = o_wbuf + NW * BPW * BSTR;
     __host__ __device__ static int in_ring_floats(int pitch) { return T * B * pitch; }
@@ -249,8 +273,8 @@ struct Layout {
     }
 };
 
-// i / n and i % n for small non-negative i, n through a float reciprocal
-// (exact while i * n < 2^22, which the shared-memory extents guarantee)
+// i / n for small non-negative i, n through a float reciprocal (exact while
+// i * n < 2^22, which the shared-memory extents guarantee)
 __device__ __forceinline__ int div_small(int i, float inv_n) { return __float2int_rz(((float)i + 0.5f) * inv_n); }
 
 // ---------------------------------------------------------------------------
@@ -343,7 +367,7 @@ __device__ __forceinline__ float row_task(float* __restrict__ wb, const float* _
     return X[0][0];
 }
 
-// sum over the B lanes (rows) of one block; lanes of a block are contiguous
+// sum over the B lanes of one block; lanes of a block are contiguous
 template <int B> __device__ __forceinline__ float block_row_sum(float v) {
 #pragma unroll
     for (int o = (B < 32 ? B : 32) / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -351,83 +375,131 @@ template <int B> __device__ __forceinline__ float block_row_sum(float v) {
 }
 
 // ---------------------------------------------------------------------------
-// column phase helpers
+// column phase
 // ---------------------------------------------------------------------------
-template <int B> __device__ __forceinline__ void ydft_fwd(float (&re)[B], float (&im)[B]) {
-    if constexpr (B == 8) cdft_8_fwd(re, im);
-    if constexpr (B == 16) cdft_16_fwd(re, im);
-    if constexpr (B == 32) cdft_32_fwd(re, im);
+template <int M> __device__ __forceinline__ void half_dft_fwd(float (&re)[M], float (&im)[M]) {
+    if constexpr (M == 4) cdft_4_fwd(re, im);
+    if constexpr (M == 8) cdft_8_fwd(re, im);
+    if constexpr (M == 16) cdft_16_fwd(re, im);
 }
-template <int B> __device__ __forceinline__ void ydft_inv(float (&re)[B], float (&im)[B]) {
-    if constexpr (B == 8) cdft_8_inv(re, im);
-    if constexpr (B == 16) cdft_16_inv(re, im);
-    if constexpr (B == 32) cdft_32_inv(re, im);
-}
-
-// register index of gain slot j in plane 0 (pairs (k, B-k), then 0 and B/2)
-template <int B> __host__ __device__ constexpr int slot0_reg(int j) {
-    return j == 0 ? 0 : (j == 1 ? B / 2 : ((j & 1) ? B - (j >> 1) : (j >> 1)));
+template <int M> __device__ __forceinline__ void half_dft_inv(float (&re)[M], float (&im)[M]) {
+    if constexpr (M == 4) cdft_4_inv(re, im);
+    if constexpr (M == 8) cdft_8_inv(re, im);
+    if constexpr (M == 16) cdft_16_inv(re, im);
 }
 
-// gain of every bin of one plane held in (re, im); slot tables are [B+2][H]
-template <int B, int FC, bool PLANE0>
-__device__ __forceinline__ void gain_plane(float (&re)[B], float (&im)[B], const float* __restrict__ sig,
-                                           const float* __restrict__ sig2, const float* __restrict__ wfe, int c,
-                                           float g, bool dual, const KernelArgs& a) {
-    constexpr int H = B / 2;
+// gain of the M bins a lane holds; slot tables are [NSLOT][B] per plane
+template <int M, int B, int FC, bool ZM>
+__device__ __forceinline__ void gain_lane_zm(float (&re)[M], float (&im)[M], const float* __restrict__ sig,
+                                             const float* __restrict__ sig2, const float* __restrict__ wfe, int w,
+                                             float g, bool dual, const KernelArgs& a) {
 #pragma unroll
-    for (int j = 0; j < B; ++j) {
-        const int r = PLANE0 ? slot0_reg<B>(j) : j;
-        const float s = sig[j * H + c];
-        const float s2 = (FC != kFilterWiener && dual) ? sig2[j * H + c] : s;
-        const float2 w = reinterpret_cast<const float2*>(wfe)[j * H + c];
-        apply_bin<FC>(re[r], im[r], s, s2, dual, w, g, a);
+    for (int j = 0; j < M; ++j) {
+        const float s = sig[j * B + w];
+        const float s2 = (FC != kFilterWiener && dual) ? sig2[j * B + w] : s;
+        const float2 wv = ZM ? reinterpret_cast<const float2*>(wfe)[j * B + w] : make_float2(0.0f, 0.0f);
+        apply_bin<FC, ZM>(re[j], im[j], s, s2, dual, wv, g, a);
     }
 }
 
-// one column task: lane (block, c) of a warp buffer block `wb`.
+template <int M, int B, int FC>
+__device__ __forceinline__ void gain_lane(float (&re)[M], float (&im)[M], const float* __restrict__ sig,
+                                          const float* __restrict__ sig2, const float* __restrict__ wfe, int w, float g,
+                                          bool dual, bool has_w, const KernelArgs& a) {
+    if (has_w)
+        gain_lane_zm<M, B, FC, true>(re, im, sig, sig2, wfe, w, g, dual, a);
+    else
+        gain_lane_zm<M, B, FC, false>(re, im, sig, sig2, wfe, w, g, dual, a);
+}
+
+// x *= (c + i s) for a compile-time constant (after unrolling) twiddle
+__device__ __forceinline__ void cmul_const(float& re, float& im, float c, float s) {
+    if (s == 0.0f) {
+        if (c != 1.0f) {
+            re *= c;
+            im *= c;
+        }
+    } else if (c == 0.0f) {
+        const float t = re;
+        re = -im * s;
+        im = t * s;
+    } else {
+        const float r = fmaf(re, c, -im * s);
+        im = fmaf(re, s, im * c);
+        re = r;
+    }
+}
+
+// In-lane partner pairs (k, -k mod B) of the y-bins k = 2m + h a lane holds:
+// h = 0: (m, M-m) for 0 < m < M/2, with m = 0 and m = M/2 self-paired;
+// h = 1: (m, M-1-m) for 0 <= m < M/2.
+template <int M, typename F>
+__device__ __forceinline__ void for_pairs(int h, F&& f) {
+    if (h == 0) {
+#pragma unroll
+        for (int m = 1; m < M / 2; ++m) f(m, M - m);
+    } else {
+#pragma unroll
+        for (int m = 0; m < M / 2; ++m) f(m, M - 1 - m);
+    }
+}
+
+// One column task: lane w = 2c + h of a block (`wb` = the block's buffer).
 //
-// Every temporal plane p is transformed along y, filtered, weighted by its
-// centre-frame twiddle w^(p r) and summed into S.  The packed lane (c = 0)
-// holds, for p <= r, the spectrum A_p of x-bin 0 and, for p > r, the
-// spectrum B_q (q = T - p) of x-bin B/2; each plane enters S through its
-// Hermitian part, the B planes multiplied by i, so that after plane 0 the
-// packed lane holds S_A + i S_B and one inverse y-DFT yields both columns.
+// Packed x-column c (c = 0 carries x-bins 0 and B/2) is split over the lane
+// pair h = 0, 1 by y-bin parity: lane h forms t[y] = (x[y] + (-1)^h x[y+M])
+// * W_B^(h y), y < M, whose M-point DFT is bins k = 2m + h (one radix-2
+// decimation-in-frequency step).  Every temporal plane is transformed,
+// filtered, weighted by its centre-frame twiddle w^(p r) and summed into S;
+// the packed lanes enter each plane through its Hermitian part (B-column
+// planes multiplied by i) so that S = S_A + i S_B.  The inverse y-DFT runs
+// per half (M points, post-twiddle W_B^(-h n)) and the halves are combined
+// with one shuffle exchange: y[n] = f0 + f1, y[n+M] = f0 - f1.
 template <int B, int T, int FC>
 __device__ __forceinline__ void column_task(float* __restrict__ wb, float g, const float* __restrict__ sm_sig,
-                                            const float* __restrict__ sm_sig2, const float* __restrict__ sm_wfe, int c,
-                                            bool dual_tables, const KernelArgs& a) {
+                                            const float* __restrict__ sm_sig2, const float* __restrict__ sm_wfe, int w,
+                                            bool dual_tables, bool store, const KernelArgs& a) {
     using TL = Tile<B>;
-    constexpr int H = B / 2;
+    constexpr int M = B / 2;
     constexpr int R = (T - 1) / 2;
-    constexpr int NSLOT = B + 2;
+    constexpr int NS = M + 2;
+    const int c = w >> 1, h = w & 1;
     const bool packed = (c == 0);
     const bool dual = dual_tables && packed;
+    const float hs = h ? -1.0f : 1.0f;
 
-    float sr[B], si[B];
+    float sr[M], si[M];
 #pragma unroll
-    for (int k = 0; k < B; ++k) sr[k] = si[k] = 0.0f;
-    float qr[B], qi[B];
+    for (int k = 0; k < M; ++k) sr[k] = si[k] = 0.0f;
+    float qr[M], qi[M];
+
+    auto load_half = [&](const float* plane) {
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+            const float2 x0 = *reinterpret_cast<const float2*>(plane + TL::off(m, 2 * c));
+            const float2 x1 = *reinterpret_cast<const float2*>(plane + TL::off(m + M, 2 * c));
+            qr[m] = fmaf(hs, x1.x, x0.x);
+            qi[m] = fmaf(hs, x1.y, x0.y);
+        }
+        if (h) {
+#pragma unroll
+            for (int m = 0; m < M; ++m) cmul_const(qr[m], qi[m], HalfTwiddle<B>::re(m), HalfTwiddle<B>::im(m));
+        }
+        half_dft_fwd<M>(qr, qi);
+    };
 
 #pragma unroll
     for (int p = 1; p < T; ++p) {
-        const float* src = wb + p * B * B;
-#pragma unroll
-        for (int y = 0; y < B; ++y) {
-            const float2 v = *reinterpret_cast<const float2*>(src + TL::off(y, 2 * c));
-            qr[y] = v.x;
-            qi[y] = v.y;
-        }
-        ydft_fwd<B>(qr, qi);
-        gain_plane<B, FC, false>(qr, qi, sm_sig + p * NSLOT * H, sm_sig2 + p * NSLOT * H, sm_wfe + 2 * p * NSLOT * H,
-                                 c, g, dual, a);
-        // twiddle: w^(p r) = (tc, ts); packed lane on a B plane uses i * conj(w^(p r))
+        load_half(wb + p * B * B);
+        gain_lane<M, B, FC>(qr, qi, sm_sig + p * NS * B, sm_sig2 + p * NS * B, sm_wfe + 2 * p * NS * B, w, g, dual,
+                            (a.wmask >> p) & 1, a);
+        // twiddle w^(p r); the packed lane on a B-column plane uses i * conj(w^(p r))
         const float tc = CentreTwiddle<T>::re(p), ts = CentreTwiddle<T>::im(p);
         const bool swap = packed && (p > R);
         const float twr = swap ? ts : tc;
         const float twi = swap ? tc : ts;
 #pragma unroll
-        for (int k = 0; k < B; ++k) {
+        for (int k = 0; k < M; ++k) {
             const float vr = fmaf(qr[k], twr, -qi[k] * twi);
             const float vi = fmaf(qr[k], twi, qi[k] * twr);
             qr[k] = vr;
@@ -436,80 +508,92 @@ __device__ __forceinline__ void column_task(float* __restrict__ wb, float g, con
         if (packed) {
             // Hermitian part (A planes) or anti-Hermitian part (i * B planes)
             const float sg = (p <= R) ? 1.0f : -1.0f;
-            qr[0] = qr[0] + sg * qr[0];
-            qi[0] = qi[0] - sg * qi[0];
-            qr[H] = qr[H] + sg * qr[H];
-            qi[H] = qi[H] - sg * qi[H];
-#pragma unroll
-            for (int k = 1; k < H; ++k) {
-                const float ar = qr[k], ai = qi[k], br = qr[B - k], bi = qi[B - k];
-                qr[k] = fmaf(sg, br, ar);
-                qi[k] = fmaf(-sg, bi, ai);
-                qr[B - k] = fmaf(sg, ar, br);
-                qi[B - k] = fmaf(-sg, ai, bi);
+            if (h == 0) {
+                qr[0] += sg * qr[0];
+                qi[0] -= sg * qi[0];
+                qr[M / 2] += sg * qr[M / 2];
+                qi[M / 2] -= sg * qi[M / 2];
             }
+            for_pairs<M>(h, [&](int i, int j) {
+                const float ar = qr[i], ai = qi[i], br = qr[j], bi = qi[j];
+                qr[i] = fmaf(sg, br, ar);
+                qi[i] = fmaf(-sg, bi, ai);
+                qr[j] = fmaf(sg, ar, br);
+                qi[j] = fmaf(-sg, ai, bi);
+            });
         }
 #pragma unroll
-        for (int k = 0; k < B; ++k) {
+        for (int k = 0; k < M; ++k) {
             sr[k] += qr[k];
             si[k] += qi[k];
         }
     }
 
     // plane 0 last
-#pragma unroll
-    for (int y = 0; y < B; ++y) {
-        const float2 v = *reinterpret_cast<const float2*>(wb + TL::off(y, 2 * c));
-        qr[y] = v.x;
-        qi[y] = v.y;
-    }
-    ydft_fwd<B>(qr, qi);
+    load_half(wb);
     float e1r = 0.0f, e1i = 0.0f, e2r = 0.0f, e2i = 0.0f;
     if (packed) {
-        // untangle Q = A + iB (A, B Hermitian): A -> reg k, B -> reg B-k
-#pragma unroll
-        for (int k = 1; k < H; ++k) {
-            const float ar = qr[k], ai = qi[k], br = qr[B - k], bi = qi[B - k];
-            qr[k] = 0.5f * (ar + br);
-            qi[k] = 0.5f * (ai - bi);
-            qr[B - k] = 0.5f * (ai + bi);
-            qi[B - k] = 0.5f * (br - ar);
+        // untangle Q = A + iB (A, B Hermitian in y): A(k) -> reg of k, B(k) -> reg of -k
+        for_pairs<M>(h, [&](int i, int j) {
+            const float ar = qr[i], ai = qi[i], br = qr[j], bi = qi[j];
+            qr[i] = 0.5f * (ar + br);
+            qi[i] = 0.5f * (ai - bi);
+            qr[j] = 0.5f * (ai + bi);
+            qi[j] = 0.5f * (br - ar);
+        });
+        if (h == 0) {
+            // bins 0 and B/2 are self-paired: A and B are the real and imaginary parts
+            e1r = qi[0];
+            e2r = qi[M / 2];
+            qi[0] = 0.0f;
+            qi[M / 2] = 0.0f;
         }
-        e1r = qr[H];
-        e2r = qi[H];
-        qr[H] = qi[0];
-        qi[H] = 0.0f;
-        qi[0] = 0.0f;
     }
-    gain_plane<B, FC, true>(qr, qi, sm_sig, sm_sig2, sm_wfe, c, g, dual, a);
+    gain_lane<M, B, FC>(qr, qi, sm_sig, sm_sig2, sm_wfe, w, g, dual, a.wmask & 1, a);
     if (packed) {
-        const float2 w1 = reinterpret_cast<const float2*>(sm_wfe)[B * H + c];
-        const float2 w2 = reinterpret_cast<const float2*>(sm_wfe)[(B + 1) * H + c];
-        apply_bin<FC>(e1r, e1i, sm_sig[B * H + c], dual ? sm_sig2[B * H + c] : 0.0f, dual, w1, g, a);
-        apply_bin<FC>(e2r, e2i, sm_sig[(B + 1) * H + c], dual ? sm_sig2[(B + 1) * H + c] : 0.0f, dual, w2, g, a);
-        // add Y_A0 + i Y_B0, both Hermitian in y
-        sr[0] += qr[0];
-        si[0] += qr[H];
-        sr[H] += e1r;
-        si[H] += e2r;
-#pragma unroll
-        for (int k = 1; k < H; ++k) {
-            const float ar = qr[k], ai = qi[k], br = qr[B - k], bi = qi[B - k];
-            sr[k] += ar - bi;
-            si[k] += ai + br;
-            sr[B - k] += ar + bi;
-            si[B - k] += br - ai;
+        if (h == 0) {
+            const float2 w1 = reinterpret_cast<const float2*>(sm_wfe)[M * B + w];
+            const float2 w2 = reinterpret_cast<const float2*>(sm_wfe)[(M + 1) * B + w];
+            apply_bin<FC>(e1r, e1i, sm_sig[M * B + w], dual ? sm_sig2[M * B + w] : 0.0f, dual, w1, g, a);
+            apply_bin<FC>(e2r, e2i, sm_sig[(M + 1) * B + w], dual ? sm_sig2[(M + 1) * B + w] : 0.0f, dual, w2, g, a);
+            sr[0] += qr[0];
+            si[0] += e1r;
+            sr[M / 2] += qr[M / 2];
+            si[M / 2] += e2r;
         }
+        // add Y_A0 + i Y_B0, both Hermitian in y
+        for_pairs<M>(h, [&](int i, int j) {
+            const float ar = qr[i], ai = qi[i], br = qr[j], bi = qi[j];
+            sr[i] += ar - bi;
+            si[i] += ai + br;
+            sr[j] += ar + bi;
+            si[j] += br - ai;
+        });
     } else {
 #pragma unroll
-        for (int k = 0; k < B; ++k) {
+        for (int k = 0; k < M; ++k) {
             sr[k] += qr[k];
             si[k] += qi[k];
         }
     }
-    ydft_inv<B>(sr, si);
+    // inverse y-DFT: M points per half, post-twiddle, combine the halves
+    half_dft_inv<M>(sr, si);
+    if (h) {
 #pragma unroll
-    for (int y = 0; y < B; ++y) *reinterpret_cast<float2*>(wb + TL::off(y, 2 * c)) = make_float2(sr[y], si[y]);
+        for (int n = 0; n < M; ++n) cmul_const(sr[n], si[n], HalfTwiddle<B>::re(n), -HalfTwiddle<B>::im(n));
+    }
+#pragma unroll
+    for (int n = 0; n < M; ++n) {
+        const float orr = __shfl_xor_sync(0xffffffffu, sr[n], 1);
+        const float oi = __shfl_xor_sync(0xffffffffu, si[n], 1);
+        sr[n] = fmaf(hs, sr[n], orr);
+        si[n] = fmaf(hs, si[n], oi);
+    }
+    if (store) {
+#pragma unroll
+        for (int n = 0; n < M; ++n)
+            *reinterpret_cast<float2*>(wb + TL::off(n + h * M, 2 * c)) = make_float2(sr[n], si[n]);
+    }
 }
 
 // inverse rows: packed row -> real, synthesis window, in place
@@ -542,12 +626,12 @@ __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefe
 // ---------------------------------------------------------------------------
 // main kernel
 // ---------------------------------------------------------------------------
-template <int B, int T, int NW, int FC>
-__global__ void __launch_bounds__(NW * 32, NW <= 4 ? 2 : 1) dfttest_unit_kernel(const __grid_constant__ KernelArgs a) {
+template <int B, int T, int NW, int FC, int MINB = 1>
+__global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __grid_constant__ KernelArgs a) {
     using L = Layout<B, T, NW>;
     using TL = Tile<B>;
-    constexpr int H = B / 2;
-    constexpr int BPW = 64 / B;
+    constexpr int M = B / 2;
+    constexpr int BPW = 32 / B;
     constexpr int BPS = NW * BPW;  // blocks per step
     constexpr int NT = NW * 32;
     extern __shared__ __align__(16) float sm[];
@@ -597,162 +681,175 @@ __global__ void __launch_bounds__(NW * 32, NW <= 4 ? 2 : 1) dfttest_unit_kernel(
     for (int i = tid; i < T * B * B; i += NT) s_win[(i / B) * TL::WP + (i % B)] = a.scale * a.win[i];
     for (int i = tid; i < B * B; i += NT) s_wsyn[(i / B) * TL::WP + (i % B)] = a.wsyn[i];
     const bool dual_tables = (FC != kFilterWiener) && a.sig2 != nullptr;
-    for (int i = tid; i < T * L::NSLOT * H; i += NT) {
+    for (int i = tid; i < T * L::NSLOT * B; i += NT) {
         s_sig[i] = a.sig[i];
         if (dual_tables) s_sig2[i] = a.sig2[i];
     }
-    for (int i = tid; i < 2 * T * L::NSLOT * H; i += NT) s_wfe[i] = a.wfe[i];
+    for (int i = tid; i < 2 * T * L::NSLOT * B; i += NT) s_wfe[i] = a.wfe[i];
     for (int i = tid; i < L::ola_floats(pitch); i += NT) s_ola[i] = 0.0f;
 
     const int fw = u.fw;
-    const int x0 = u.bx0 * S;  // footprint origin (padded coordinates)
+    const int x0 = u.bx0 * S;            // footprint origin (padded coordinates)
+    const int rowlen = nbx * S + O;      // footprint width
     const bool vec = ((S & 3) == 0);
-    const float inv_fw = 1.0f / (float)fw;
+    const int excl_y0 = u.by0 * S + O, excl_y1 = u.by1 * S;
+    const int excl_x0 = x0 + O, excl_x1 = u.bx1 * S;
 
-    for (int by = u.by0; by <= u.by1; ++by) {
-        // ---- finalize rows of the previous step + stage input rows of this one
-        if (by > u.by0) {
-            const int pb = by - 1;
-            const bool last = (pb == u.by1 - 1);
-            const int nrows = last ? B : S;
-            const int excl_y0 = u.by0 * S + O, excl_y1 = u.by1 * S;
-            const int excl_x0 = x0 + O, excl_x1 = u.bx1 * S;
-            for (int i = tid; i < nrows * fw; i += NT) {
-                const int r = div_small(i, inv_fw);
-                const int lx = i - r * fw;
-                const int py = pb * S + r;
-                float* cell = s_ola + (py % B) * pitch + lx;
-                const float v = *cell;
-                *cell = 0.0f;
-                const int px = x0 + lx;
-                if (px < ox || px >= ox + W || py < oy || py >= oy + Hh) continue;
-                const bool excl = (px >= excl_x0) && (px < excl_x1) && (py >= excl_y0) && (py < excl_y1);
-                if (excl) {
-                    store_sample(job.dst, (long long)(py - oy) * job.dst_stride + (px - ox), v, a.kind, a.scale,
-                                 a.peak, is_float ? 0.0f : inv_scale);
-                } else {
-                    rec[band_index(lx, py - u.by0 * S, fw, u.fh, O)] = v;
-                }
-            }
+    // input rows [r_lo, r_lo + nr) of every temporal plane: element i of the
+    // flattened (t, row, x) range -> (plane, ring offset, global index)
+    const int esz = a.kind == kF32 ? 4 : (a.kind == kU16 ? 2 : 1);
+    auto stage_item = [&](int i, int r_lo, int nr, float inv_nr_rl, float inv_rl, int& t, int& soff, long long& gidx) {
+        t = div_small(i, inv_nr_rl);
+        const int rem = i - t * nr * rowlen;
+        const int r = div_small(rem, inv_rl);
+        const int lx = rem - r * rowlen;
+        const int py = r_lo + r;
+        soff = (t * B + (py % B)) * pitch + lx;
+        gidx = (long long)mirror(py - oy, Hh) * job.src_stride + mirror(x0 + lx - ox, W);
+    };
+    const float inv_rl = 1.0f / (float)rowlen;
+    const float inv_S = 1.0f / (float)S;
+    // prologue: the first B rows of the unit
+    {
+        const int nr = B;
+        const float inv_nr_rl = 1.0f / (float)(nr * rowlen);
+        for (int i = tid; i < T * nr * rowlen; i += NT) {
+            int t, soff;
+            long long gidx;
+            stage_item(i, u.by0 * S, nr, inv_nr_rl, inv_rl, t, soff, gidx);
+            s_in[soff] = load_sample(job.src[t], gidx, a.kind);
         }
-        if (by == u.by1) break;
-        {
-            const int r_lo = (by == u.by0) ? by * S : by * S + B - S;
-            const int r_hi = by * S + B;
-            const int nr = r_hi - r_lo;
-            const int rowlen = nbx * S + O;  // footprint width of this step
-            for (int row = warp; row < T * nr; row += NW) {
-                const int t = row / nr;
-                const int py = r_lo + (row - t * nr);
-                const long long sy_ = mirror(py - oy, Hh);
-                const void* base = job.src[t];
-                for (int lx = lane; lx < rowlen; lx += 32) {
-                    const int sx_ = mirror(x0 + lx - ox, W);
-                    s_in[(t * B + (py % B)) * pitch + lx] = load_sample(base, sy_ * job.src_stride + sx_, a.kind);
-                }
-            }
-            // warm L2 with the rows of the next step (one request per 128 B)
-            if (by + 1 < u.by1) {
-                const int npy = r_hi;  // first new row of the next step
-                const int esz = a.kind == kF32 ? 4 : (a.kind == kU16 ? 2 : 1);
-                const int sx_lo = max(x0 - ox, 0), sx_hi = max(min(x0 + rowlen - ox, W) - 1, sx_lo);
-                const int nline = (int)(((long long)(sx_hi - sx_lo) * esz) / 128) + 2;
-                for (int i = tid; i < T * S * nline; i += NT) {
-                    const int t = i / (S * nline);
-                    const int rem = i - t * S * nline;
-                    const int r = rem / nline, li = rem - r * nline;
-                    const int py = npy + r;
-                    if (py >= ph) continue;
-                    const long long sy_ = mirror(py - oy, Hh);
-                    const int sxp = min(sx_lo + li * (128 / esz), sx_hi);
-                    prefetch_l2(reinterpret_cast<const char*>(job.src[t]) + (sy_ * job.src_stride + sxp) * esz);
-                }
-            }
-        }
-        __syncthreads();
+    }
 
-        // ---- per-warp block transforms
+    // lane roles: rows (b, y) and columns (b, w = 2c + h), B lanes per block
+    const int lb = lane / B, lw = lane % B;
+    const int bl = warp * BPW + lb;  // local block index of this lane
+    float* wbl = s_wbuf + bl * L::BSTR;
+    const bool valid = bl < nbx;
+    const int blr = valid ? bl : nbx - 1;
+    constexpr int PF = 4;  // input samples per thread carried in registers across the overlap-add
+
+    for (int by = u.by0; by < u.by1; ++by) {
+        __syncthreads();  // input rows of this step staged; block buffers free
+
+        // ---- per-warp block transforms (B lanes per block, BPW blocks per warp)
         {
-            float* wb0 = s_wbuf + warp * BPW * L::BSTR;
-            // row phase: 2 tasks per lane; the DC of each block is summed
-            // over its rows with shuffles (lanes of a block are contiguous)
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const int gr = k * 32 + lane;
-                const int b = gr / B, y = gr % B;
-                const int bl = warp * BPW + b;
-                const bool valid = bl < nbx;
-                const int blr = valid ? bl : nbx - 1;
-                const float dc = row_task<B, T>(wb0 + b * L::BSTR, s_in, pitch, (by * S + y) % B, blr * S, s_win, y,
-                                                vec, valid);
-                const float tot = block_row_sum<B>(dc);
-                // g = DC / Re(WF[0]) (cpu_source/kernel.hpp:1945)
-                if (y == 0 && valid) s_g[warp * BPW + b] = a.g_div != 0.0f ? __fdiv_rn(tot, a.g_div) : 0.0f;
-            }
+            // row phase: the DC of each block is summed over its rows with shuffles
+            const float dc = row_task<B, T>(wbl, s_in, pitch, (by * S + lw) % B, blr * S, s_win, lw, vec, valid);
+            const float tot = block_row_sum<B>(dc);
+            // g = DC / Re(WF[0]) (cpu_source/kernel.hpp:1945)
+            if (lw == 0 && valid) s_g[bl] = a.g_div != 0.0f ? __fdiv_rn(tot, a.g_div) : 0.0f;
             __syncwarp();
-            {
-                const int b = lane / H, c = lane % H;
-                const int bl = warp * BPW + b;
-                if (bl < nbx)
-                    column_task<B, T, FC>(wb0 + b * L::BSTR, s_g[warp * BPW + b], s_sig, s_sig2, s_wfe, c, dual_tables,
-                                          a);
-            }
+            column_task<B, T, FC>(wbl, s_g[bl], s_sig, s_sig2, s_wfe, lw, dual_tables, valid, a);
             __syncwarp();
+            if (valid) inverse_row_task<B>(wbl, s_wsyn, lw);
+        }
+        __syncthreads();  // block outputs complete; this step's input rows consumed
+
+        const bool last = (by + 1 == u.by1);
+        // ---- next step's new input rows: loads issued now, stored after the overlap-add
+        const int n_lo = (by + 1) * S + B - S;
+        const int n_items = last ? 0 : T * S * rowlen;
+        const float inv_nr_rl = 1.0f / (float)(S * rowlen);
+        unsigned pf[PF];
+        int pf_off[PF];
 #pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const int gr = k * 32 + lane;
-                const int b = gr / B, y = gr % B;
-                const int bl = warp * BPW + b;
-                if (bl < nbx) inverse_row_task<B>(wb0 + b * L::BSTR, s_wsyn, y);
+        for (int k = 0; k < PF; ++k) {
+            const int i = tid + k * NT;
+            pf_off[k] = -1;
+            if (i < n_items) {
+                int t;
+                long long gidx;
+                stage_item(i, n_lo, S, inv_nr_rl, inv_rl, t, pf_off[k], gidx);
+                pf[k] = load_raw(job.src[t], gidx, a.kind);
             }
         }
-        __syncthreads();
 
-        // ---- overlap-add: every ring pixel sums the blocks covering it
-        {
-            const int rowlen = nbx * S + O;
-            if (vec) {
-                const int nq = rowlen >> 2;
-                const float inv_nq = 1.0f / (float)nq;
-                for (int i = tid; i < B * nq; i += NT) {
-                    const int r = div_small(i, inv_nq), q = i - r * nq;
-                    const int px = 4 * q;
-                    int b_lo = px - B + 4;
-                    b_lo = b_lo <= 0 ? 0 : (b_lo + S - 1) / S;
-                    int b_hi = px / S;
-                    b_hi = b_hi < nbx - 1 ? b_hi : nbx - 1;
-                    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-                    for (int bl = b_lo; bl <= b_hi; ++bl) {
-                        const float* ob = s_wbuf + bl * L::BSTR;
-                        const float4 v = *reinterpret_cast<const float4*>(ob + TL::off(r, px - bl * S));
-                        acc.x += v.x;
-                        acc.y += v.y;
-                        acc.z += v.z;
-                        acc.w += v.w;
-                    }
-                    float4* cell = reinterpret_cast<float4*>(s_ola + ((by * S + r) % B) * pitch + px);
-                    float4 c4 = *cell;
-                    c4.x += acc.x;
-                    c4.y += acc.y;
-                    c4.z += acc.z;
-                    c4.w += acc.w;
-                    *cell = c4;
-                }
+        // ---- overlap-add of this step's blocks into the ring; rows that no
+        // later block reaches are final and leave the ring (same thread, no barrier)
+        const int nfin = last ? B : S;
+        auto finish = [&](int py, int lx, float v) {
+            const int px = x0 + lx;
+            if (px < ox || px >= ox + W || py < oy || py >= oy + Hh) return;
+            if (px >= excl_x0 && px < excl_x1 && py >= excl_y0 && py < excl_y1) {
+                store_sample(job.dst, (long long)(py - oy) * job.dst_stride + (px - ox), v, a.kind, a.scale, a.peak,
+                             is_float ? 0.0f : inv_scale);
             } else {
-                const float inv_rl = 1.0f / (float)rowlen;
-                for (int i = tid; i < B * rowlen; i += NT) {
-                    const int r = div_small(i, inv_rl), px = i - r * rowlen;
-                    int b_lo = px - B + 1;
-                    b_lo = b_lo <= 0 ? 0 : (b_lo + S - 1) / S;
-                    int b_hi = px / S;
-                    b_hi = b_hi < nbx - 1 ? b_hi : nbx - 1;
-                    float acc = 0.0f;
-                    for (int bl = b_lo; bl <= b_hi; ++bl) acc += s_wbuf[bl * L::BSTR + TL::off(r, px - bl * S)];
-                    s_ola[((by * S + r) % B) * pitch + px] += acc;
+                rec[band_index(lx, py - u.by0 * S, fw, u.fh, O)] = v;
+            }
+        };
+        if (vec) {
+            const int nq = rowlen >> 2;
+            const float inv_nq = 1.0f / (float)nq;
+            for (int i = tid; i < B * nq; i += NT) {
+                const int r = div_small(i, inv_nq), q = i - r * nq;
+                const int px = 4 * q;
+                // blocks k with k*S <= px <= k*S + B - 4
+                const int b_lo = px <= B - 4 ? 0 : div_small(px - B + 3 + S, inv_S);
+                const int b_hi = min(div_small(px, inv_S), nbx - 1);
+                const int py = by * S + r;
+                float4* cell = reinterpret_cast<float4*>(s_ola + (py % B) * pitch + px);
+                float4 acc = *cell;
+                for (int k = b_lo; k <= b_hi; ++k) {
+                    const float4 v = *reinterpret_cast<const float4*>(s_wbuf + k * L::BSTR + TL::off(r, px - k * S));
+                    acc.x += v.x;
+                    acc.y += v.y;
+                    acc.z += v.z;
+                    acc.w += v.w;
                 }
+                if (r < nfin) {
+                    finish(py, px, acc.x);
+                    finish(py, px + 1, acc.y);
+                    finish(py, px + 2, acc.z);
+                    finish(py, px + 3, acc.w);
+                    acc = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+                *cell = acc;
+            }
+        } else {
+            for (int i = tid; i < B * rowlen; i += NT) {
+                const int r = div_small(i, inv_rl), px = i - r * rowlen;
+                // blocks k with k*S <= px <= k*S + B - 1
+                const int b_lo = px <= B - 1 ? 0 : div_small(px - B + S, inv_S);
+                const int b_hi = min(div_small(px, inv_S), nbx - 1);
+                const int py = by * S + r;
+                float* cell = s_ola + (py % B) * pitch + px;
+                float acc = *cell;
+                for (int k = b_lo; k <= b_hi; ++k) acc += s_wbuf[k * L::BSTR + TL::off(r, px - k * S)];
+                if (r < nfin) {
+                    finish(py, px, acc);
+                    acc = 0.0f;
+                }
+                *cell = acc;
             }
         }
-        __syncthreads();
+
+        // ---- store the prefetched rows (and any beyond the register budget)
+#pragma unroll
+        for (int k = 0; k < PF; ++k)
+            if (pf_off[k] >= 0) s_in[pf_off[k]] = raw_to_float(pf[k], a.kind);
+        for (int i = tid + PF * NT; i < n_items; i += NT) {
+            int t, soff;
+            long long gidx;
+            stage_item(i, n_lo, S, inv_nr_rl, inv_rl, t, soff, gidx);
+            s_in[soff] = load_sample(job.src[t], gidx, a.kind);
+        }
+        // warm L2 with the rows of the step after next (one request per 128 B)
+        if (by + 2 < u.by1) {
+            const int npy = n_lo + S;
+            const int sx_lo = max(x0 - ox, 0), sx_hi = max(min(x0 + rowlen - ox, W) - 1, sx_lo);
+            const int nline = (int)(((long long)(sx_hi - sx_lo) * esz) / 128) + 2;
+            for (int i = tid; i < T * S * nline; i += NT) {
+                const int t = i / (S * nline);
+                const int rem = i - t * S * nline;
+                const int r = rem / nline, li = rem - r * nline;
+                const int py = npy + r;
+                if (py >= ph) continue;
+                const long long sy_ = mirror(py - oy, Hh);
+                const int sxp = min(sx_lo + li * (128 / esz), sx_hi);
+                prefetch_l2(reinterpret_cast<const char*>(job.src[t]) + (sy_ * job.src_stride + sxp) * esz);
+            }
+        }
     }
 }
 

@@ -396,6 +396,8 @@ def all_codelets():
         out.append(("c2r", n, gen_c2r(n)))
         out.append(("cdft_fwd", n, gen_cdft(n, -1)))
         out.append(("cdft_inv", n, gen_cdft(n, +1)))
+    out.append(("cdft_fwd", 4, gen_cdft(4, -1)))
+    out.append(("cdft_inv", 4, gen_cdft(4, +1)))
     for n in (3, 5, 7):
         out.append(("cdft_fwd", n, gen_cdft(n, -1)))
         out.append(("rdftT", n, gen_rdft_odd(n)))
@@ -432,9 +434,29 @@ def twiddle_tables():
     return lines
 
 
+def half_twiddle_tables():
+    """W_B^(-y) = exp(-2 pi i y / B), y < B/2: the pre-twiddle of the odd
+    half of a radix-2 decimation-in-frequency split (its conjugate is the
+    inverse post-twiddle)."""
+    lines = ["template <int B> struct HalfTwiddle;"]
+    for B in (8, 16, 32):
+        M = B // 2
+        re = [math.cos(2 * math.pi * y / B) for y in range(M)]
+        im = [-math.sin(2 * math.pi * y / B) for y in range(M)]
+        fix = lambda v: 0.0 if abs(v) < 1e-15 else v
+        re_s = ", ".join(_f32(fix(v)) for v in re)
+        im_s = ", ".join(_f32(fix(v)) for v in im)
+        lines.append(f"template <> struct HalfTwiddle<{B}> {{")
+        lines.append(f"    static __device__ __forceinline__ float re(int y) {{ constexpr float v[{M}] = {{{re_s}}}; return v[y]; }}")
+        lines.append(f"    static __device__ __forceinline__ float im(int y) {{ constexpr float v[{M}] = {{{im_s}}}; return v[y]; }}")
+        lines.append("};")
+    return lines
+
+
 def write(path):
     parts = [HEADER]
     parts += twiddle_tables()
+    parts += half_twiddle_tables()
     parts.append("")
     for kind, n, (sig, lines, counts) in all_codelets():
         parts.append(f"// {kind} n={n}: {counts['add']} add, {counts['fma']} fma, {counts['mul']} mul")
