@@ -122,6 +122,32 @@ int dfttest2_b200_process_clip_host(dfttest2_b200_filter* f, const void* src, pt
                                     ptrdiff_t dst_frame_bytes, int nframes, int width, int height, int sample_type,
                                     int bits_per_sample);
 
+/* Size of the device array that dfttest2_b200_process_plane_noalloc works
+ * in (bytes, per GPU, held from library load until process exit). */
+#define DFTTEST2_B200_NOALLOC_SCRATCH_BYTES (8u * 1024u * 1024u)
+
+/* Allocation-free single-plane filter.  No counterpart in the reference:
+ * this is an addition for callers that cannot allocate GPU memory, such as
+ * a host that hands the filter frames from a memory pool it has already
+ * reserved and that must not see cudaMalloc / cudaFree (which can claim
+ * memory outside its budget and implicitly synchronise the device in the
+ * middle of its pipeline).
+ *
+ * It takes the DFTTest arguments (as dfttest2_b200_create) and one plane
+ * whose pointers are device memory on params->device_id, and queues the
+ * same kernels as dfttest2_b200_process_planes on `stream`, asynchronously.
+ * It allocates nothing: its tables, plane descriptor and overlap scratch
+ * live in one statically sized device array of
+ * DFTTEST2_B200_NOALLOC_SCRATCH_BYTES; a plane whose scratch needs more is
+ * rejected with an error that states both sizes.
+ *
+ * The first call on a device resolves the array's device address; make
+ * that first call before any stream capture.  All calls on a device share
+ * the array, so calls that overlap on the GPU (different streams, or
+ * concurrent host threads) race: serialise them on one stream. */
+int dfttest2_b200_process_plane_noalloc(const dfttest2_b200_params* params, const dfttest2_b200_plane* plane,
+                                        int sample_type, int bits_per_sample, void* stream);
+
 /* RDFT: FP64 direct real DFT over 1, 2 or 3 axes, real last axis first
  * (cpu_source/source.cpp:269-340).  `out` receives
  * prod(shape[:-1]) * (shape[-1]/2+1) interleaved (re, im) values. */

@@ -745,3 +745,248 @@ const char* dfttest2_b200_version(void) {
 const char* dfttest2_b200_last_error(void) { return g_last_error.c_str(); }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point (dfttest2_b200_process_plane_noalloc)
+//
+// For hosts that cannot allocate GPU memory: everything the kernels need
+// besides the caller's planes (tables, the plane descriptor, the error flag
+// and the per-unit overlap bands) is placed in one file-scope device array.
+// In host code `g_noalloc_scratch` is only a stand-in symbol; its device
+// address comes from cudaGetSymbolAddress, once per device.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocBytes = DFTTEST2_B200_NOALLOC_SCRATCH_BYTES;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_lock;
+unsigned char* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// device address of the array on the current device `dev` (set-up on first use)
+int noalloc_address(int dev, unsigned char** out) {
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(DFTTEST2_B200_EINVAL, "invalid device_id");
+    std::lock_guard<std::mutex> lk(g_noalloc_lock);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(DFTTEST2_B200_ECUDA, std::string("cudaGetSymbolAddress of the scratch array failed: ") +
+                                                 cudaGetErrorString(e));
+        g_noalloc_addr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return 0;
+}
+
+size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+// fixed-capacity tables (T <= 7, B <= 32), built on the host stack
+struct NoAllocTables {
+    float win[7 * 32 * 32];
+    float wsyn[32 * 32];
+    float sig[7 * 18 * 32];
+    float sig2[7 * 18 * 32];
+    float wfe[2 * 7 * 18 * 32];
+};
+
+}  // namespace
+
+extern "C" int dfttest2_b200_process_plane_noalloc(const dfttest2_b200_params* p, const dfttest2_b200_plane* plane,
+                                                   int sample_type, int bits_per_sample, void* stream) {
+    if (!p || !plane) return fail(DFTTEST2_B200_EINVAL, "null argument");
+    // argument checks of DFTTestCreate (nvrtc_source/source.cpp:650-760)
+    const int radius = p->radius < 0 ? 0 : p->radius;
+    if (p->radius > 3) return fail(DFTTEST2_B200_EINVAL, "\"radius\" must be in [0, 1, 2, 3]");
+    const int B = p->block_size < 0 ? 16 : p->block_size;
+    if (B != 8 && B != 16 && B != 32) return fail(DFTTEST2_B200_EINVAL, "\"block_size\" must be 8, 16 or 32");
+    const int S = p->block_step < 0 ? B : p->block_step;
+    if (S < 1 || S > B) return fail(DFTTEST2_B200_EINVAL, "\"block_step\" must be in [1, block_size]");
+    const int T = 2 * radius + 1, H = B / 2, X = H + 1, M = B / 2, NS = M + 2, O = B - S;
+    const int zero_mean = p->zero_mean < 0 ? 1 : !!p->zero_mean;
+    const int device_id = p->device_id < 0 ? 0 : p->device_id;
+    if (p->filter_type < 0 || p->filter_type > 6) return fail(DFTTEST2_B200_EINVAL, "\"filter_type\" must be in [0, 6]");
+    if (p->window_len != T * B * B || !p->window) return fail(DFTTEST2_B200_EINVAL, "invalid window size");
+    if (p->sigma_len <= 0 || !p->sigma) return fail(DFTTEST2_B200_EINVAL, "sigma must not be empty");
+    if (p->sigma_len != 1 && p->sigma_len != T * B * X) return fail(DFTTEST2_B200_EINVAL, "invalid sigma array size");
+    if (zero_mean && (p->window_freq_len != T * B * X * 2 || !p->window_freq))
+        return fail(DFTTEST2_B200_EINVAL, "invalid window_freq size");
+    const int syn = p->synthesis_slice < 0 ? radius : p->synthesis_slice;
+    if (syn >= T) return fail(DFTTEST2_B200_EINVAL, "\"synthesis_slice\" out of range");
+    if (int rc = check_format(sample_type, bits_per_sample)) return rc;
+    const Variant var = select_variant(B, T);
+    if (!var.main) return fail(DFTTEST2_B200_EINVAL, "unsupported block_size / radius");
+
+    // -- tables (same layout as dfttest2_b200_create builds) -----------------
+    NoAllocTables tb;
+    for (int i = 0; i < T * B * B; ++i) tb.win[i] = (float)p->window[i];
+    for (int i = 0; i < B * B; ++i) tb.wsyn[i] = tb.win[syn * B * B + i];
+    auto sigma_at = [&](int t, int y, int x) -> float {
+        return p->sigma_len == 1 ? (float)p->sigma[0] : (float)p->sigma[(t * B + y) * X + x];
+    };
+    auto wf_at = [&](int t, int y, int x, int part) -> float {
+        return zero_mean ? (float)p->window_freq[((t * B + y) * X + x) * 2 + part] : 0.0f;
+    };
+    bool asym = false;
+    auto put = [&](int pl, int j, int w, int t, int y, int x, int t2, int y2) {
+        const int idx = (pl * NS + j) * B + w;
+        tb.sig[idx] = sigma_at(t, y, x);
+        tb.sig2[idx] = sigma_at(t2, y2, x);
+        tb.wfe[2 * idx] = wf_at(t, y, x, 0);
+        tb.wfe[2 * idx + 1] = wf_at(t, y, x, 1);
+        if (tb.sig2[idx] != tb.sig[idx]) asym = true;
+    };
+    auto neg = [&](int k) { return (B - k) % B; };
+    for (int pl = 0; pl < T; ++pl) {
+        for (int w = 0; w < B; ++w) {
+            const int c = w >> 1, h = w & 1;
+            for (int j = 0; j < NS; ++j) put(pl, j, w, 0, 0, 0, 0, 0);
+            if (c > 0) {
+                for (int m = 0; m < M; ++m) put(pl, m, w, pl, 2 * m + h, c, pl, 2 * m + h);
+                continue;
+            }
+            if (pl > 0) {
+                for (int m = 0; m < M; ++m) {
+                    const int k = 2 * m + h;
+                    if (pl <= radius) put(pl, m, w, pl, k, 0, T - pl, neg(k));
+                    else put(pl, m, w, T - pl, k, H, pl, neg(k));
+                }
+                continue;
+            }
+            if (h == 0) {
+                put(0, 0, w, 0, 0, 0, 0, 0);
+                put(0, M / 2, w, 0, H, 0, 0, H);
+                for (int m = 1; m < M / 2; ++m) {
+                    put(0, m, w, 0, 2 * m, 0, 0, neg(2 * m));
+                    put(0, M - m, w, 0, 2 * m, H, 0, neg(2 * m));
+                }
+                put(0, M, w, 0, 0, H, 0, 0);
+                put(0, M + 1, w, 0, H, H, 0, H);
+            } else {
+                for (int m = 0; m < M / 2; ++m) {
+                    put(0, m, w, 0, 2 * m + 1, 0, 0, neg(2 * m + 1));
+                    put(0, M - 1 - m, w, 0, 2 * m + 1, H, 0, neg(2 * m + 1));
+                }
+            }
+        }
+    }
+    int wmask = 0;
+    for (int pl = 0; pl < T; ++pl)
+        for (int i = 0; i < NS * B * 2; ++i)
+            if (tb.wfe[pl * NS * B * 2 + i] != 0.0f) wmask |= 1 << pl;
+    const float g_div = zero_mean ? (float)p->window_freq[0] : 0.0f;
+    if (zero_mean && g_div == 0.0f) return fail(DFTTEST2_B200_EINVAL, "window_freq[0] must be non-zero");
+
+    // -- the plane and its unit split ------------------------------------------
+    const int bps = bytes_of(sample_type, bits_per_sample);
+    const int pw = dft2::pad_size(plane->width, B, S), ph = dft2::pad_size(plane->height, B, S);
+    const int ox = (pw - plane->width) / 2, oy = (ph - plane->height) / 2;
+    if (plane->width <= std::max(ox, pw - plane->width - ox) || plane->height <= std::max(oy, ph - plane->height - oy))
+        return fail(DFTTEST2_B200_EINVAL, "plane too small for the block size");
+    for (int t = 0; t < T; ++t)
+        if (!plane->src[t]) return fail(DFTTEST2_B200_EINVAL, "null source plane");
+    if (!plane->dst) return fail(DFTTEST2_B200_EINVAL, "null destination plane");
+    if (plane->src_stride % bps || plane->dst_stride % bps || plane->src_stride < (ptrdiff_t)plane->width * bps ||
+        plane->dst_stride < (ptrdiff_t)plane->width * bps)
+        return fail(DFTTEST2_B200_EINVAL, "invalid stride");
+
+    DeviceGuard dg(device_id);
+    int dev = -1, num_sms = 148;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev != device_id) return fail(DFTTEST2_B200_EINVAL, "invalid device_id");
+    CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+
+    const int BPS = var.nw * var.bpw;
+    const int pnx = dft2::pad_num(plane->width, B, S), pny = dft2::pad_num(plane->height, B, S);
+    const int nsx = (pnx + BPS - 1) / BPS;
+    const int min_seg = std::max((O + S - 1) / S, 4);
+    const size_t off_err = 0, off_job = 256;
+    const size_t off_win = align256(off_job + sizeof(dft2::PlaneJob));
+    const size_t off_wsyn = align256(off_win + sizeof(float) * T * B * B);
+    const size_t off_sig = align256(off_wsyn + sizeof(float) * B * B);
+    const size_t off_sig2 = align256(off_sig + sizeof(float) * T * NS * B);
+    const size_t off_wfe = align256(off_sig2 + sizeof(float) * T * NS * B);
+    const size_t off_band = align256(off_wfe + sizeof(float) * 2 * T * NS * B);
+    auto band_bytes = [&](int nsy, int& rec) {
+        const int wmax = (pnx + nsx - 1) / nsx, hmax = (pny + nsy - 1) / nsy;
+        rec = std::max(dft2::band_record_size(wmax * S + O, hmax * S + O, O), 1);
+        return sizeof(float) * (size_t)nsx * nsy * rec;
+    };
+    // as many segments as fill the GPU, fewer if the overlap bands must fit the array
+    int nsy = std::max(1, std::min((4 * num_sms + nsx - 1) / nsx, pny / min_seg));
+    int rec = 0;
+    while (nsy > 1 && off_band + band_bytes(nsy, rec) > kNoAllocBytes) --nsy;
+    const size_t need = off_band + band_bytes(nsy, rec);
+    if (need > kNoAllocBytes)
+        return fail(DFTTEST2_B200_EINVAL, "plane too large for the allocation-free path: needs " +
+                                              std::to_string(need) + " bytes of scratch, the array holds " +
+                                              std::to_string(kNoAllocBytes));
+
+    dft2::PlaneJob job;
+    std::memset(&job, 0, sizeof(job));
+    for (int t = 0; t < T; ++t) job.src[t] = plane->src[t];
+    job.dst = plane->dst;
+    job.src_stride = plane->src_stride / bps;
+    job.dst_stride = plane->dst_stride / bps;
+    job.width = plane->width;
+    job.height = plane->height;
+    job.nsx = nsx;
+    job.nsy = nsy;
+    job.unit_base = 0;
+    job.fix_base = 0;
+
+    unsigned char* base = nullptr;
+    if (int rc = noalloc_address(dev, &base)) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    // the error flag must start at zero; tables and the descriptor are copied
+    // in (pageable sources are staged before these calls return)
+    CUDA_TRY(cudaMemsetAsync(base + off_err, 0, sizeof(int), st));
+    CUDA_TRY(cudaMemcpyAsync(base + off_job, &job, sizeof(job), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(base + off_win, tb.win, sizeof(float) * T * B * B, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(base + off_wsyn, tb.wsyn, sizeof(float) * B * B, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(base + off_sig, tb.sig, sizeof(float) * T * NS * B, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(base + off_sig2, tb.sig2, sizeof(float) * T * NS * B, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(base + off_wfe, tb.wfe, sizeof(float) * 2 * T * NS * B, cudaMemcpyHostToDevice, st));
+
+    float scale, peak;
+    int kind;
+    scale_peak(sample_type, bits_per_sample, scale, peak, kind);
+    dft2::KernelArgs a{};
+    a.jobs = reinterpret_cast<const dft2::PlaneJob*>(base + off_job);
+    a.njobs = 1;
+    a.nunits = nsx * nsy;
+    a.nfix = (nsx - 1) * O * plane->height + (nsy - 1) * O * plane->width;
+    a.kind = kind;
+    a.scale = scale;
+    a.peak = peak;
+    a.block_step = S;
+    a.filter_type = p->filter_type;
+    a.sigma2 = (float)p->sigma2;
+    a.pmin = (float)p->pmin;
+    a.pmax = (float)p->pmax;
+    a.g_div = g_div;
+    a.win = reinterpret_cast<const float*>(base + off_win);
+    a.wsyn = reinterpret_cast<const float*>(base + off_wsyn);
+    a.sig = reinterpret_cast<const float*>(base + off_sig);
+    a.sig2 = asym ? reinterpret_cast<const float*>(base + off_sig2) : nullptr;
+    a.wfe = reinterpret_cast<const float*>(base + off_wfe);
+    a.wmask = zero_mean ? wmask : 0;
+    a.scratch = reinterpret_cast<float*>(base + off_band);
+    a.rec_stride = rec;
+    a.ring_pitch = ((BPS * S + O) + 3) & ~3;
+    a.error_flag = reinterpret_cast<int*>(base + off_err);
+
+    const size_t smem = var.smem(a.ring_pitch);
+    KernelFn kern = (p->filter_type == 0 && !asym) ? var.main : var.generic;
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<a.nunits, var.nw * 32, smem, st>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    if (a.nfix > 0) {
+        const int threads = 256;
+        const int blocks = std::min((a.nfix + threads - 1) / threads, num_sms * 8);
+        var.fixup<<<blocks, threads, 0, st>>>(a);
+        CUDA_TRY(cudaGetLastError());
+    }
+    return 0;
+}

@@ -13,6 +13,7 @@ from ctypes import POINTER, c_char_p, c_double, c_int, c_ssize_t, c_void_p
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libdfttest2_b200.so")
 
+NOALLOC_SCRATCH_BYTES = 8 * 1024 * 1024
 OK = 0
 EINVAL = 1
 ECUDA = 2
@@ -66,6 +67,7 @@ SIGNATURES = {
         c_int,
         [c_void_p, c_void_p, c_ssize_t, c_ssize_t, c_void_p, c_ssize_t, c_ssize_t, c_int, c_int, c_int, c_int, c_int],
     ),
+    "dfttest2_b200_process_plane_noalloc": (c_int, [POINTER(Params), POINTER(Plane), c_int, c_int, c_void_p]),
     "dfttest2_b200_rdft": (c_int, [POINTER(c_double), c_int, POINTER(c_int), c_int, POINTER(c_double), c_int]),
     "dfttest2_b200_version": (c_char_p, []),
     "dfttest2_b200_last_error": (c_char_p, []),
