@@ -305,19 +305,24 @@ def main():
     def step():
         flt.process_planes_device(planes, 0, 16, stream.cuda_stream)
 
+    clocks = ClockSampler(local).__enter__()  # started early: nvidia-smi takes a moment to produce samples
     for _ in range(opts.warmup):
         step()
     torch.cuda.synchronize()
+    time.sleep(0.5)
     if pg:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
-        start.record(stream)
-        for _ in range(opts.steps):
-            step()
-        stop.record(stream)
-        torch.cuda.synchronize()
+    n_before = len(clocks.lines)
+    start.record(stream)
+    for _ in range(opts.steps):
+        step()
+    stop.record(stream)
+    torch.cuda.synchronize()
+    time.sleep(0.2)
+    clocks.__exit__(None, None, None)
+    clocks.lines = clocks.lines[n_before:] or clocks.lines
     ms = start.elapsed_time(stop)
     if pg:
         torch.distributed.barrier()

@@ -114,6 +114,11 @@ Variant select_variant(int B, int T) {
 struct Slot {
     cudaEvent_t done = nullptr;
     cudaStream_t stream = nullptr;        // own stream (host paths)
+    cudaStream_t up = nullptr;            // host -> device copies of the clip path
+    cudaStream_t down = nullptr;          // device -> host copies of the clip path
+    cudaEvent_t ev_up[2] = {};
+    cudaEvent_t ev_comp[2] = {};
+    cudaEvent_t ev_down[2] = {};
     dft2::PlaneJob* d_jobs = nullptr;
     size_t jobs_cap = 0;
     float* d_scratch = nullptr;
@@ -388,6 +393,13 @@ void free_filter(dfttest2_b200_filter* f) {
         if (s.d_frames) cudaFree(s.d_frames);
         if (s.h_pinned) cudaFreeHost(s.h_pinned);
         if (s.stream) cudaStreamDestroy(s.stream);
+        if (s.up) cudaStreamDestroy(s.up);
+        if (s.down) cudaStreamDestroy(s.down);
+        for (int k = 0; k < 2; ++k) {
+            if (s.ev_up[k]) cudaEventDestroy(s.ev_up[k]);
+            if (s.ev_comp[k]) cudaEventDestroy(s.ev_comp[k]);
+            if (s.ev_down[k]) cudaEventDestroy(s.ev_down[k]);
+        }
         if (s.done) cudaEventDestroy(s.done);
     }
     cudaFree(f->d_win);
@@ -553,6 +565,13 @@ int dfttest2_b200_create(const dfttest2_b200_params* p, dfttest2_b200_filter** o
         Slot& s = f->slots[i];
         CUDA_TRY(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
         CUDA_TRY(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaStreamCreateWithFlags(&s.up, cudaStreamNonBlocking));
+        CUDA_TRY(cudaStreamCreateWithFlags(&s.down, cudaStreamNonBlocking));
+        for (int k = 0; k < 2; ++k) {
+            CUDA_TRY(cudaEventCreateWithFlags(&s.ev_up[k], cudaEventDisableTiming));
+            CUDA_TRY(cudaEventCreateWithFlags(&s.ev_comp[k], cudaEventDisableTiming));
+            CUDA_TRY(cudaEventCreateWithFlags(&s.ev_down[k], cudaEventDisableTiming));
+        }
         CUDA_TRY(cudaMalloc((void**)&s.d_error, sizeof(int)));
         CUDA_TRY(cudaMemset(s.d_error, 0, sizeof(int)));
         CUDA_TRY(cudaEventRecord(s.done, s.stream));
@@ -637,26 +656,30 @@ int dfttest2_b200_process_clip_host(dfttest2_b200_filter* f, const void* src, pt
     const int r = f->radius;
     SlotGuard sg(f);
     Slot& s = sg.slot();
-    // chunked pipeline: every source frame is uploaded once into a dense
-    // device array; a chunk of outputs is filtered with one launch
-    const int chunk = std::max(1, std::min(nframes, 32));
-    if (int rc = ensure_bytes(s.d_frames, s.frames_cap, frame * ((size_t)nframes + chunk), s.done)) return rc;
+    // Three-stream pipeline over chunks of output frames: uploads (stream
+    // `up`), filtering (slot stream) and downloads (stream `down`) of
+    // consecutive chunks overlap.  Every source frame is uploaded once into a
+    // dense device array; outputs alternate between two chunk buffers.
+    const int chunk = std::max(1, std::min(nframes, 16));
+    if (int rc = ensure_bytes(s.d_frames, s.frames_cap, frame * ((size_t)nframes + 2 * chunk), s.done)) return rc;
     CUDA_TRY(cudaEventSynchronize(s.done));
     uint8_t* dframes = (uint8_t*)s.d_frames;
-    uint8_t* dout = dframes + frame * nframes;
+    uint8_t* dout[2] = {dframes + frame * nframes, dframes + frame * ((size_t)nframes + chunk)};
     const uint8_t* hsrc = (const uint8_t*)src;
     uint8_t* hdst = (uint8_t*)dst;
     float scale, peak;
     int kind;
     scale_peak(sample_type, bits_per_sample, scale, peak, kind);
     int uploaded = 0;
-    for (int c0 = 0; c0 < nframes; c0 += chunk) {
+    int k = 0;
+    for (int c0 = 0; c0 < nframes; c0 += chunk, ++k) {
         const int c1 = std::min(nframes, c0 + chunk);
         const int need = std::min(nframes, c1 + r);
         for (; uploaded < need; ++uploaded) {
             CUDA_TRY(cudaMemcpy2DAsync(dframes + frame * uploaded, row, hsrc + src_frame_bytes * uploaded, src_stride,
-                                       row, height, cudaMemcpyHostToDevice, s.stream));
+                                       row, height, cudaMemcpyHostToDevice, s.up));
         }
+        CUDA_TRY(cudaEventRecord(s.ev_up[k & 1], s.up));
         std::vector<dfttest2_b200_plane> planes(c1 - c0);
         for (int n = c0; n < c1; ++n) {
             dfttest2_b200_plane& p = planes[n - c0];
@@ -666,21 +689,27 @@ int dfttest2_b200_process_clip_host(dfttest2_b200_filter* f, const void* src, pt
                 p.src[t] = dframes + frame * fi;
             }
             p.src_stride = row;
-            p.dst = dout + frame * (n - c0);
+            p.dst = dout[k & 1] + frame * (n - c0);
             p.dst_stride = row;
             p.width = width;
             p.height = height;
         }
         Plan plan;
         if (int rc = make_plan(f, planes.data(), (int)planes.size(), bps, plan)) return rc;
+        CUDA_TRY(cudaStreamWaitEvent(s.stream, s.ev_up[k & 1], 0));
+        if (k >= 2) CUDA_TRY(cudaStreamWaitEvent(s.stream, s.ev_down[k & 1], 0));  // output buffer free
         if (int rc = launch(f, s, plan, kind, scale, peak, s.stream)) return rc;
+        CUDA_TRY(cudaEventRecord(s.ev_comp[k & 1], s.stream));
+        CUDA_TRY(cudaStreamWaitEvent(s.down, s.ev_comp[k & 1], 0));
         for (int n = c0; n < c1; ++n) {
-            CUDA_TRY(cudaMemcpy2DAsync(hdst + dst_frame_bytes * n, dst_stride, dout + frame * (n - c0), row, row,
-                                       height, cudaMemcpyDeviceToHost, s.stream));
+            CUDA_TRY(cudaMemcpy2DAsync(hdst + dst_frame_bytes * n, dst_stride, dout[k & 1] + frame * (n - c0), row, row,
+                                       height, cudaMemcpyDeviceToHost, s.down));
         }
-        CUDA_TRY(cudaEventRecord(s.done, s.stream));
-        CUDA_TRY(cudaEventSynchronize(s.done));
+        CUDA_TRY(cudaEventRecord(s.ev_down[k & 1], s.down));
     }
+    CUDA_TRY(cudaStreamSynchronize(s.down));
+    CUDA_TRY(cudaStreamSynchronize(s.stream));
+    CUDA_TRY(cudaEventRecord(s.done, s.stream));
     return 0;
 }
 
