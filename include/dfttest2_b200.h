@@ -122,6 +122,37 @@ int dfttest2_b200_process_clip_host(dfttest2_b200_filter* f, const void* src, pt
                                     ptrdiff_t dst_frame_bytes, int nframes, int width, int height, int sample_type,
                                     int bits_per_sample);
 
+/* Differentiable path (float planes).  The reference has no gradient; these
+ * serve training the sigma array and backpropagating through the filter.
+ *
+ * dfttest2_b200_process_planes_sigma: as dfttest2_b200_process_planes, with
+ * the per-bin sigma array taken from device memory (float,
+ * (2r+1)*B*(B/2+1), layout of the `sigma` argument), so it can change
+ * between calls without host round trips.
+ *
+ * dfttest2_b200_backward_planes: adjoint of the same filter.  For every
+ * plane, grad_dst is dL/d(output plane); dL/d(source planes) is ADDED to
+ * grad_src[t] (the caller zeroes them; planes that alias the same frame
+ * accumulate) and dL/d(sigma) is ADDED to grad_sigma (may be NULL).  sigma
+ * NULL means the array given at create time.  Block spectra are recomputed,
+ * nothing is kept from the forward call. */
+typedef struct dfttest2_b200_grad_plane {
+    const void* src[7];
+    float* grad_src[7];
+    const float* grad_dst;
+    ptrdiff_t src_stride;
+    ptrdiff_t grad_src_stride;
+    ptrdiff_t grad_dst_stride;
+    int width;
+    int height;
+} dfttest2_b200_grad_plane;
+
+int dfttest2_b200_process_planes_sigma(dfttest2_b200_filter* f, const dfttest2_b200_plane* planes, int nplanes,
+                                       int sample_type, int bits_per_sample, const float* sigma, void* stream);
+
+int dfttest2_b200_backward_planes(dfttest2_b200_filter* f, const dfttest2_b200_grad_plane* planes, int nplanes,
+                                  const float* sigma, float* grad_sigma, void* stream);
+
 /* Size of the device array that dfttest2_b200_process_plane_noalloc works
  * in (bytes, per GPU, held from library load until process exit). */
 #define DFTTEST2_B200_NOALLOC_SCRATCH_BYTES (8u * 1024u * 1024u)

@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <climits>
 #include <cmath>
 #include <complex>
 #include <condition_variable>
@@ -25,6 +26,7 @@
 
 #include "dfttest2_b200.h"
 #include "dfttest_kernel.cuh"
+#include "dfttest_adjoint.cuh"
 
 #ifndef DFTTEST2_B200_VERSION
 #define DFTTEST2_B200_VERSION "0.1.0"
@@ -129,6 +131,10 @@ struct Slot {
     size_t frames_cap = 0;
     void* h_pinned = nullptr;
     size_t pinned_cap = 0;
+    float* d_sigtab = nullptr;       // gain-slot sigma tables built from a device sigma array
+    size_t sigtab_cap = 0;
+    dft2::GradJob* d_gjobs = nullptr;
+    size_t gjobs_cap = 0;
 };
 
 }  // namespace
@@ -151,6 +157,12 @@ struct dfttest2_b200_filter {
     float* d_sig2 = nullptr;
     float* d_wfe = nullptr;
     int wmask = 0;
+    // differentiable path: full (t, y, x) arrays and the gain-slot -> bin maps
+    float* d_sigma_full = nullptr;  // [T][B][X]
+    float* d_wf_full = nullptr;     // [T][B][X][2]
+    int* d_sig_idx = nullptr;       // [T][B/2+2][B]
+    int* d_sig2_idx = nullptr;
+    int n_slots = 0;
 
     std::vector<Slot> slots;
     std::vector<int> free_slots;
@@ -310,7 +322,7 @@ int make_plan(const dfttest2_b200_filter* f, const dfttest2_b200_plane* planes, 
 }
 
 int launch(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, float scale, float peak,
-           cudaStream_t stream) {
+           cudaStream_t stream, const float* sig_override = nullptr, const float* sig2_override = nullptr) {
     if (plan.nunits == 0) return 0;
     CUDA_TRY(cudaStreamWaitEvent(stream, slot.done, 0));
     if (int rc = ensure(slot.d_jobs, slot.jobs_cap, plan.jobs.size(), slot.done)) return rc;
@@ -335,8 +347,8 @@ int launch(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, floa
     a.g_div = f->zero_mean ? f->g_div : 0.0f;
     a.win = f->d_win;
     a.wsyn = f->d_wsyn;
-    a.sig = f->d_sig;
-    a.sig2 = f->asym ? f->d_sig2 : nullptr;
+    a.sig = sig_override ? sig_override : f->d_sig;
+    a.sig2 = sig_override ? sig2_override : (f->asym ? f->d_sig2 : nullptr);
     a.wfe = f->d_wfe;
     a.wmask = f->zero_mean ? f->wmask : 0;
     a.scratch = slot.d_scratch;
@@ -345,7 +357,7 @@ int launch(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, floa
     a.error_flag = slot.d_error;
 
     const size_t smem = f->var.smem(plan.pitch);
-    KernelFn kern = (f->filter_type == 0 && !f->asym) ? f->var.main : f->var.generic;
+    KernelFn kern = (f->filter_type == 0 && !f->asym && !sig_override) ? f->var.main : f->var.generic;
     CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<plan.nunits, f->var.nw * 32, smem, stream>>>(a);
     CUDA_TRY(cudaGetLastError());
@@ -382,6 +394,52 @@ void scale_peak(int sample_type, int bits, float& scale, float& peak, int& kind)
     }
 }
 
+template <int B, int T>
+int launch_adjoint_t(dft2::AdjointArgs a, int num_sms, cudaStream_t st) {
+    using L = dft2::AdjTile<B, T>;
+    a.patch_h = B + (L::TBY - 1) * a.block_step;
+    a.patch_w = B + (L::TBX - 1) * a.block_step;
+    const size_t smem = L::smem_bytes(a.patch_h, a.patch_w);
+    auto kern = dft2::dfttest_adjoint_kernel<B, T>;
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, L::NTH, smem));
+    if (per_sm < 1) return fail(DFTTEST2_B200_ECUDA, "adjoint kernel does not fit on an SM");
+    const int grid = std::max(1, std::min(a.ntiles, num_sms * per_sm));
+    kern<<<grid, L::NTH, smem, st>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+template <int B, int T>
+void adjoint_tile_dims_t(int& tbx, int& tby) {
+    tbx = dft2::AdjTile<B, T>::TBX;
+    tby = dft2::AdjTile<B, T>::TBY;
+}
+
+#define DFT2_FOR_ADJ_VARIANTS(M) M(16, 1) M(16, 3) M(16, 5) M(16, 7)
+#ifndef DFTTEST2_B200_ONLY_B16
+#define DFT2_FOR_ADJ_MORE(M) M(8, 1) M(8, 3) M(8, 5) M(8, 7) M(32, 1) M(32, 3) M(32, 5) M(32, 7)
+#else
+#define DFT2_FOR_ADJ_MORE(M)
+#endif
+
+int adjoint_tile_dims(int B, int T, int& tbx, int& tby) {
+#define DFT2_ADJ(b, t) \
+    if (B == b && T == t) return adjoint_tile_dims_t<b, t>(tbx, tby), 0;
+    DFT2_FOR_ADJ_VARIANTS(DFT2_ADJ) DFT2_FOR_ADJ_MORE(DFT2_ADJ)
+#undef DFT2_ADJ
+    return fail(DFTTEST2_B200_EINVAL, "unsupported block_size / radius");
+}
+
+int launch_adjoint(int B, int T, const dft2::AdjointArgs& a, int num_sms, cudaStream_t st) {
+#define DFT2_ADJ(b, t) \
+    if (B == b && T == t) return launch_adjoint_t<b, t>(a, num_sms, st);
+    DFT2_FOR_ADJ_VARIANTS(DFT2_ADJ) DFT2_FOR_ADJ_MORE(DFT2_ADJ)
+#undef DFT2_ADJ
+    return fail(DFTTEST2_B200_EINVAL, "unsupported block_size / radius");
+}
+
 void free_filter(dfttest2_b200_filter* f) {
     if (!f) return;
     DeviceGuard g(f->device);
@@ -391,6 +449,8 @@ void free_filter(dfttest2_b200_filter* f) {
         if (s.d_scratch) cudaFree(s.d_scratch);
         if (s.d_error) cudaFree(s.d_error);
         if (s.d_frames) cudaFree(s.d_frames);
+        if (s.d_sigtab) cudaFree(s.d_sigtab);
+        if (s.d_gjobs) cudaFree(s.d_gjobs);
         if (s.h_pinned) cudaFreeHost(s.h_pinned);
         if (s.stream) cudaStreamDestroy(s.stream);
         if (s.up) cudaStreamDestroy(s.up);
@@ -407,6 +467,10 @@ void free_filter(dfttest2_b200_filter* f) {
     cudaFree(f->d_sig);
     cudaFree(f->d_sig2);
     cudaFree(f->d_wfe);
+    cudaFree(f->d_sigma_full);
+    cudaFree(f->d_wf_full);
+    cudaFree(f->d_sig_idx);
+    cudaFree(f->d_sig2_idx);
     delete f;
 }
 
@@ -490,9 +554,12 @@ int dfttest2_b200_create(const dfttest2_b200_params* p, dfttest2_b200_filter** o
     // sigma of the Hermitian partner bin (t, -k) of packed-column bins.
     const int M = B / 2, NS = M + 2;
     std::vector<float> sig(T * NS * B), sig2(T * NS * B), wfe(2 * T * NS * B);
+    std::vector<int> sig_idx(T * NS * B), sig2_idx(T * NS * B);
     bool asym = false;
     auto put = [&](int pl, int j, int w, int t, int y, int x, int t2, int y2) {
         const int idx = (pl * NS + j) * B + w;
+        sig_idx[idx] = (t * B + y) * X + x;
+        sig2_idx[idx] = (t2 * B + y2) * X + x;
         sig[idx] = sigma_at(t, y, x);
         sig2[idx] = sigma_at(t2, y2, x);
         wfe[2 * idx] = wf_at(t, y, x, 0);
@@ -559,6 +626,22 @@ int dfttest2_b200_create(const dfttest2_b200_params* p, dfttest2_b200_filter** o
     if (int rc = upload(f->d_sig, sig)) return rc;
     if (int rc = upload(f->d_sig2, sig2)) return rc;
     if (int rc = upload(f->d_wfe, wfe)) return rc;
+    {
+        std::vector<float> sfull(T * B * X), wffull(2 * T * B * X, 0.0f);
+        for (int t = 0; t < T; ++t)
+            for (int y = 0; y < B; ++y)
+                for (int x = 0; x < X; ++x) {
+                    const int i = (t * B + y) * X + x;
+                    sfull[i] = sigma_at(t, y, x);
+                    wffull[2 * i] = wf_at(t, y, x, 0);
+                    wffull[2 * i + 1] = wf_at(t, y, x, 1);
+                }
+        if (int rc = upload(f->d_sigma_full, sfull)) return rc;
+        if (int rc = upload(f->d_wf_full, wffull)) return rc;
+        if (int rc = upload(f->d_sig_idx, sig_idx)) return rc;
+        if (int rc = upload(f->d_sig2_idx, sig2_idx)) return rc;
+        f->n_slots = T * NS * B;
+    }
 
     f->slots.resize(num_streams);
     for (int i = 0; i < num_streams; ++i) {
@@ -710,6 +793,94 @@ int dfttest2_b200_process_clip_host(dfttest2_b200_filter* f, const void* src, pt
     CUDA_TRY(cudaStreamSynchronize(s.down));
     CUDA_TRY(cudaStreamSynchronize(s.stream));
     CUDA_TRY(cudaEventRecord(s.done, s.stream));
+    return 0;
+}
+
+int dfttest2_b200_process_planes_sigma(dfttest2_b200_filter* f, const dfttest2_b200_plane* planes, int nplanes,
+                                       int sample_type, int bits_per_sample, const float* sigma, void* stream) {
+    if (!f) return fail(DFTTEST2_B200_EINVAL, "null filter");
+    if (!sigma) return fail(DFTTEST2_B200_EINVAL, "null sigma");
+    if (nplanes < 0 || (nplanes > 0 && !planes)) return fail(DFTTEST2_B200_EINVAL, "invalid plane list");
+    if (int rc = check_format(sample_type, bits_per_sample)) return rc;
+    DeviceGuard dg(f->device);
+    Plan plan;
+    if (int rc = make_plan(f, planes, nplanes, bytes_of(sample_type, bits_per_sample), plan)) return rc;
+    float scale, peak;
+    int kind;
+    scale_peak(sample_type, bits_per_sample, scale, peak, kind);
+    SlotGuard sg(f);
+    Slot& s = sg.slot();
+    cudaStream_t st = (cudaStream_t)stream;
+    CUDA_TRY(cudaStreamWaitEvent(st, s.done, 0));
+    if (int rc = ensure(s.d_sigtab, s.sigtab_cap, (size_t)2 * f->n_slots, s.done)) return rc;
+    dft2::sigma_tables_kernel<<<(f->n_slots + 255) / 256, 256, 0, st>>>(sigma, f->d_sig_idx, f->d_sig2_idx, s.d_sigtab,
+                                                                       s.d_sigtab + f->n_slots, f->n_slots);
+    CUDA_TRY(cudaGetLastError());
+    return launch(f, s, plan, kind, scale, peak, st, s.d_sigtab, s.d_sigtab + f->n_slots);
+}
+
+int dfttest2_b200_backward_planes(dfttest2_b200_filter* f, const dfttest2_b200_grad_plane* planes, int nplanes,
+                                  const float* sigma, float* grad_sigma, void* stream) {
+    if (!f) return fail(DFTTEST2_B200_EINVAL, "null filter");
+    if (nplanes < 0 || (nplanes > 0 && !planes)) return fail(DFTTEST2_B200_EINVAL, "invalid plane list");
+    if (nplanes == 0) return 0;
+    DeviceGuard dg(f->device);
+    const int B = f->B, S = f->S, T = f->T;
+    int tbx, tby;
+    if (int rc = adjoint_tile_dims(B, T, tbx, tby)) return rc;
+    std::vector<dft2::GradJob> jobs(nplanes);
+    long long ntiles = 0;
+    for (int i = 0; i < nplanes; ++i) {
+        const dfttest2_b200_grad_plane& p = planes[i];
+        const int pw = dft2::pad_size(p.width, B, S), ph = dft2::pad_size(p.height, B, S);
+        const int ox = (pw - p.width) / 2, oy = (ph - p.height) / 2;
+        if (p.width <= std::max(ox, pw - p.width - ox) || p.height <= std::max(oy, ph - p.height - oy))
+            return fail(DFTTEST2_B200_EINVAL, "plane too small for the block size");
+        if (!p.grad_dst) return fail(DFTTEST2_B200_EINVAL, "null output gradient");
+        if (p.src_stride % 4 || p.grad_src_stride % 4 || p.grad_dst_stride % 4)
+            return fail(DFTTEST2_B200_EINVAL, "invalid stride");
+        dft2::GradJob& j = jobs[i];
+        std::memset(&j, 0, sizeof(j));
+        for (int t = 0; t < T; ++t) {
+            if (!p.src[t] || !p.grad_src[t]) return fail(DFTTEST2_B200_EINVAL, "null source plane");
+            j.src[t] = (const float*)p.src[t];
+            j.gsrc[t] = p.grad_src[t];
+        }
+        j.gdst = p.grad_dst;
+        j.src_stride = p.src_stride / 4;
+        j.gsrc_stride = p.grad_src_stride / 4;
+        j.gdst_stride = p.grad_dst_stride / 4;
+        j.width = p.width;
+        j.height = p.height;
+        j.tile_base = (int)ntiles;
+        j.ntx = (dft2::pad_num(p.width, B, S) + tbx - 1) / tbx;
+        ntiles += (long long)j.ntx * ((dft2::pad_num(p.height, B, S) + tby - 1) / tby);
+        if (ntiles > INT_MAX) return fail(DFTTEST2_B200_EINVAL, "too many planes in one call");
+    }
+    SlotGuard sg(f);
+    Slot& s = sg.slot();
+    cudaStream_t st = (cudaStream_t)stream;
+    CUDA_TRY(cudaStreamWaitEvent(st, s.done, 0));
+    if (int rc = ensure(s.d_gjobs, s.gjobs_cap, jobs.size(), s.done)) return rc;
+    CUDA_TRY(cudaMemcpyAsync(s.d_gjobs, jobs.data(), jobs.size() * sizeof(dft2::GradJob), cudaMemcpyHostToDevice, st));
+    dft2::AdjointArgs a{};
+    a.jobs = s.d_gjobs;
+    a.njobs = nplanes;
+    a.ntiles = (int)ntiles;
+    a.scale = 255.0f;
+    a.block_step = S;
+    a.filter_type = f->filter_type;
+    a.sigma2 = f->sigma2;
+    a.pmin = f->pmin;
+    a.pmax = f->pmax;
+    a.zero_mean = f->zero_mean ? 1 : 0;
+    a.win = f->d_win;
+    a.wsyn = f->d_wsyn;
+    a.sigma = sigma ? sigma : f->d_sigma_full;
+    a.wf = f->d_wf_full;
+    a.gsigma = grad_sigma;
+    if (int rc = launch_adjoint(B, T, a, f->num_sms, st)) return rc;
+    CUDA_TRY(cudaEventRecord(s.done, st));
     return 0;
 }
 

@@ -650,7 +650,12 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
         const int mid = (lo + hi + 1) >> 1;
         if (a.jobs[mid].unit_base <= uid) lo = mid; else hi = mid - 1;
     }
-    const PlaneJob& job = a.jobs[lo];
+    // the plane descriptor is read many times per step: keep it on chip
+    __shared__ PlaneJob s_job;
+    if (tid < (int)(sizeof(PlaneJob) / sizeof(int)))
+        reinterpret_cast<int*>(&s_job)[tid] = reinterpret_cast<const int*>(&a.jobs[lo])[tid];
+    __syncthreads();
+    const PlaneJob& job = s_job;
     const int W = job.width, Hh = job.height;
     const int pw = pad_size(W, B, S), ph = pad_size(Hh, B, S);
     const int pnx = (pw - B) / S + 1, pny = (ph - B) / S + 1;
@@ -779,30 +784,27 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
             }
         };
         if (vec) {
-            const int nq = rowlen >> 2;
+            // items are pixel pairs (S, B multiples of 4: a pair never straddles a block edge)
+            const int nq = rowlen >> 1;
             const float inv_nq = 1.0f / (float)nq;
             for (int i = tid; i < B * nq; i += NT) {
                 const int r = div_small(i, inv_nq), q = i - r * nq;
-                const int px = 4 * q;
-                // blocks k with k*S <= px <= k*S + B - 4
-                const int b_lo = px <= B - 4 ? 0 : div_small(px - B + 3 + S, inv_S);
+                const int px = 2 * q;
+                // blocks k with k*S <= px <= k*S + B - 2
+                const int b_lo = px <= B - 2 ? 0 : div_small(px - B + 1 + S, inv_S);
                 const int b_hi = min(div_small(px, inv_S), nbx - 1);
                 const int py = by * S + r;
-                float4* cell = reinterpret_cast<float4*>(s_ola + (py % B) * pitch + px);
-                float4 acc = *cell;
+                float2* cell = reinterpret_cast<float2*>(s_ola + (py % B) * pitch + px);
+                float2 acc = *cell;
                 for (int k = b_lo; k <= b_hi; ++k) {
-                    const float4 v = *reinterpret_cast<const float4*>(s_wbuf + k * L::BSTR + TL::off(r, px - k * S));
+                    const float2 v = *reinterpret_cast<const float2*>(s_wbuf + k * L::BSTR + TL::off(r, px - k * S));
                     acc.x += v.x;
                     acc.y += v.y;
-                    acc.z += v.z;
-                    acc.w += v.w;
                 }
                 if (r < nfin) {
                     finish(py, px, acc.x);
                     finish(py, px + 1, acc.y);
-                    finish(py, px + 2, acc.z);
-                    finish(py, px + 3, acc.w);
-                    acc = make_float4(0.f, 0.f, 0.f, 0.f);
+                    acc = make_float2(0.f, 0.f);
                 }
                 *cell = acc;
             }

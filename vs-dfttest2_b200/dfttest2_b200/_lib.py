@@ -56,6 +56,19 @@ class Plane(ctypes.Structure):
     ]
 
 
+class GradPlane(ctypes.Structure):
+    _fields_ = [
+        ("src", c_void_p * 7),
+        ("grad_src", c_void_p * 7),
+        ("grad_dst", c_void_p),
+        ("src_stride", c_ssize_t),
+        ("grad_src_stride", c_ssize_t),
+        ("grad_dst_stride", c_ssize_t),
+        ("width", c_int),
+        ("height", c_int),
+    ]
+
+
 # every symbol include/dfttest2_b200.h declares, with its ctypes signature
 SIGNATURES = {
     "dfttest2_b200_params_init": (None, [POINTER(Params)]),
@@ -67,6 +80,8 @@ SIGNATURES = {
         c_int,
         [c_void_p, c_void_p, c_ssize_t, c_ssize_t, c_void_p, c_ssize_t, c_ssize_t, c_int, c_int, c_int, c_int, c_int],
     ),
+    "dfttest2_b200_process_planes_sigma": (c_int, [c_void_p, POINTER(Plane), c_int, c_int, c_int, c_void_p, c_void_p]),
+    "dfttest2_b200_backward_planes": (c_int, [c_void_p, POINTER(GradPlane), c_int, c_void_p, c_void_p, c_void_p]),
     "dfttest2_b200_process_plane_noalloc": (c_int, [POINTER(Params), POINTER(Plane), c_int, c_int, c_void_p]),
     "dfttest2_b200_rdft": (c_int, [POINTER(c_double), c_int, POINTER(c_int), c_int, POINTER(c_double), c_int]),
     "dfttest2_b200_version": (c_char_p, []),
