@@ -153,6 +153,55 @@ int dfttest2_b200_process_planes_sigma(dfttest2_b200_filter* f, const dfttest2_b
 int dfttest2_b200_backward_planes(dfttest2_b200_filter* f, const dfttest2_b200_grad_plane* planes, int nplanes,
                                   const float* sigma, float* grad_sigma, void* stream);
 
+/* Multi-clip batches.  The reference filters one clip per filter instance,
+ * one frame per DFTTestGetFrame call (nvrtc_source/source.cpp:356-605); a
+ * batch filters many device-resident clips, each with its own DFTTest
+ * arguments (its filter), size, length and sample format, in one CUDA graph
+ * launch.
+ *
+ * At creation every frame of every clip becomes a plane job of a work-list.
+ * Jobs are grouped by kernel (block size, block step, temporal size, Wiener
+ * or general gain); each group is one kernel over its cost-ordered
+ * work-list (largest planes first) plus its overlap fix-up, and the groups
+ * run as parallel branches of one graph.  With DFTTEST2_B200_BATCH_TUNE the
+ * kernel shape (warps per CTA) and unit split of every group are chosen by
+ * timing the candidates on the batch itself (the timed runs write the same
+ * outputs as a normal run); choices are cached per process by group
+ * signature.  Without it the single-call heuristics are used. */
+typedef struct dfttest2_b200_batch dfttest2_b200_batch;
+
+typedef struct dfttest2_b200_clip {
+    dfttest2_b200_filter* filter;  /* DFTTest arguments of this clip; must outlive the batch */
+    const void* src;               /* device memory: frame i at src + i*src_frame_bytes */
+    ptrdiff_t src_stride;          /* bytes between rows */
+    ptrdiff_t src_frame_bytes;
+    void* dst;                     /* device memory, same layout rules */
+    ptrdiff_t dst_stride;
+    ptrdiff_t dst_frame_bytes;
+    int nframes;                   /* the temporal window is clamped at the clip ends */
+    int width;
+    int height;
+    int sample_type;
+    int bits_per_sample;
+} dfttest2_b200_clip;
+
+#define DFTTEST2_B200_BATCH_TUNE 1
+
+/* Validates the clips (all filters on one device), builds the work-lists,
+ * tunes when asked, allocates the scratch and captures the graph.  The
+ * clip memory must stay valid for the life of the batch. */
+int dfttest2_b200_batch_create(const dfttest2_b200_clip* clips, int nclips, int flags, dfttest2_b200_batch** out);
+
+/* Launches the batch's graph on `stream` (asynchronous). */
+int dfttest2_b200_batch_run(dfttest2_b200_batch* b, void* stream);
+
+/* Writes a one-line-per-group description (kernel, shape, units, jobs, tuning
+ * times) into buf (NUL-terminated, truncated to len).  Returns the number of
+ * kernel launches per run, or a negative status. */
+int dfttest2_b200_batch_describe(const dfttest2_b200_batch* b, char* buf, int len);
+
+void dfttest2_b200_batch_free(dfttest2_b200_batch* b);
+
 /* Size of the device array that dfttest2_b200_process_plane_noalloc works
  * in (bytes, per GPU, held from library load until process exit). */
 #define DFTTEST2_B200_NOALLOC_SCRATCH_BYTES (8u * 1024u * 1024u)

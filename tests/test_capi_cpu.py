@@ -82,3 +82,28 @@ def test_plugin_plane_checks():
     kw = _base()
     with pytest.raises(_lib.Error, match="plane index out of range"):
         dfttest2_b200.DFTTest(clip, planes=[1], **kw)
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """sizeof / offsetof of every C-ABI struct (compiled from the header with
+    gcc) equal the ctypes mirrors the Python side passes."""
+    import subprocess
+
+    structs = {"dfttest2_b200_params": _lib.Params, "dfttest2_b200_plane": _lib.Plane,
+               "dfttest2_b200_grad_plane": _lib.GradPlane, "dfttest2_b200_clip": _lib.Clip}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "dfttest2_b200.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname}.{fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                        check=True).stdout.splitlines())
+    for cname, py in structs.items():
+        assert int(got[cname]) == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert int(got[f"{cname}.{fname}"]) == getattr(py, fname).offset, (cname, fname)

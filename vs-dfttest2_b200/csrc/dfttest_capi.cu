@@ -22,6 +22,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "dfttest2_b200.h"
@@ -58,6 +59,7 @@ struct Variant {
     KernelFn fixup = nullptr;
     int nw = 0;      // warps per CTA
     int bpw = 0;     // blocks per warp
+    int minb = 1;    // CTAs per SM the register budget is sized for
     size_t (*smem)(int pitch) = nullptr;
 };
 
@@ -69,6 +71,7 @@ Variant make_variant() {
     v.fixup = dft2::dfttest_fixup_kernel<B>;
     v.nw = NW;
     v.bpw = 32 / B;
+    v.minb = MINB;
     v.smem = [](int pitch) { return dft2::Layout<B, T, NW>::smem_bytes(pitch); };
     return v;
 }
@@ -111,6 +114,24 @@ Variant select_variant(int B, int T) {
 #endif
     }
     return Variant{};
+}
+
+// Kernel shapes the batch autotuner may time besides select_variant's
+// choice: other warp counts per CTA for the block sizes and temporal sizes of
+// multi-clip batches (fewer warps per CTA = narrower strips, more CTAs).
+std::vector<Variant> candidate_variants(int B, int T) {
+    std::vector<Variant> v;
+    v.push_back(select_variant(B, T));
+    if (!v.back().main) return {};
+#ifndef DFTTEST2_B200_ONLY_B16
+    if (B == 8 && T == 1) v.push_back(make_variant<8, 1, 8, 2>());
+    if (B == 8 && T == 3) v.push_back(make_variant<8, 3, 8, 2>());
+    if (B == 32 && T == 1) v.push_back(make_variant<32, 1, 8>());
+    if (B == 32 && T == 3) v.push_back(make_variant<32, 3, 4, 2>());
+#endif
+    if (B == 16 && T == 1) v.push_back(make_variant<16, 1, 8, 2>());
+    if (B == 16 && T == 3) v.push_back(make_variant<16, 3, 16>());
+    return v;
 }
 
 struct Slot {
@@ -259,33 +280,29 @@ struct Plan {
     int pitch = 0;
 };
 
-int make_plan(const dfttest2_b200_filter* f, const dfttest2_b200_plane* planes, int n, int bps_bytes, Plan& plan) {
-    const int B = f->B, S = f->S, O = B - S;
-    const int BPS = f->var.nw * f->var.bpw;
+// a plane in the work-list: strides in elements, `param` indexes per-job formats and filters
+struct PlaneRef {
+    const void* src[7];
+    void* dst;
+    long long src_stride, dst_stride;
+    int width, height;
+    int param;
+};
+
+// Unit split and work-list of planes that share (B, S) and a kernel shape of
+// BPS blocks per step: strips of at most BPS blocks; each strip is cut into
+// segments until the launch has about `target` units (segments no shorter
+// than max(O/S, 4) blocks).
+void plan_units(int B, int S, int BPS, const std::vector<PlaneRef>& planes, long long target, Plan& plan) {
+    const int O = B - S;
+    const int n = (int)planes.size();
     plan.jobs.resize(n);
-    // strips: BPS blocks at most; segments only when the launch is small
     long long strips_total = 0;
     int max_pny = 0;
-    for (int i = 0; i < n; ++i) {
-        const dfttest2_b200_plane& p = planes[i];
-        const int pw = dft2::pad_size(p.width, B, S), ph = dft2::pad_size(p.height, B, S);
-        const int ox = (pw - p.width) / 2, oy = (ph - p.height) / 2;
-        // the mirror padding must stay inside the plane
-        // (cpu_source/getframe_impl.cpp:44-62 reads 2*ox - x)
-        if (p.width <= std::max(ox, pw - p.width - ox) || p.height <= std::max(oy, ph - p.height - oy))
-            return fail(DFTTEST2_B200_EINVAL, "plane too small for the block size");
-        const int pnx = dft2::pad_num(p.width, B, S);
-        strips_total += (pnx + BPS - 1) / BPS;
+    for (const PlaneRef& p : planes) {
+        strips_total += (dft2::pad_num(p.width, B, S) + BPS - 1) / BPS;
         max_pny = std::max(max_pny, dft2::pad_num(p.height, B, S));
-        for (int t = 0; t < f->T; ++t) {
-            if (p.src[t] == nullptr) return fail(DFTTEST2_B200_EINVAL, "null source plane");
-        }
-        if (!p.dst) return fail(DFTTEST2_B200_EINVAL, "null destination plane");
-        if (p.src_stride % bps_bytes || p.dst_stride % bps_bytes || p.src_stride < (ptrdiff_t)p.width * bps_bytes ||
-            p.dst_stride < (ptrdiff_t)p.width * bps_bytes)
-            return fail(DFTTEST2_B200_EINVAL, "invalid stride");
     }
-    const long long target = 4LL * f->num_sms;
     int nsy = 1;
     if (strips_total < target) nsy = (int)((target + strips_total - 1) / strips_total);
     const int min_seg = std::max((O + S - 1) / S, 4);
@@ -293,15 +310,16 @@ int make_plan(const dfttest2_b200_filter* f, const dfttest2_b200_plane* planes, 
 
     int unit = 0, fix = 0, rec = 0;
     for (int i = 0; i < n; ++i) {
-        const dfttest2_b200_plane& p = planes[i];
+        const PlaneRef& p = planes[i];
         dft2::PlaneJob& j = plan.jobs[i];
         std::memset(&j, 0, sizeof(j));
-        for (int t = 0; t < f->T; ++t) j.src[t] = p.src[t];
+        for (int t = 0; t < 7; ++t) j.src[t] = p.src[t];
         j.dst = p.dst;
-        j.src_stride = p.src_stride / bps_bytes;
-        j.dst_stride = p.dst_stride / bps_bytes;
+        j.src_stride = p.src_stride;
+        j.dst_stride = p.dst_stride;
         j.width = p.width;
         j.height = p.height;
+        j.param = p.param;
         const int pnx = dft2::pad_num(p.width, B, S), pny = dft2::pad_num(p.height, B, S);
         j.nsx = (pnx + BPS - 1) / BPS;
         j.nsy = std::max(1, std::min(nsy, pny / min_seg));
@@ -318,6 +336,38 @@ int make_plan(const dfttest2_b200_filter* f, const dfttest2_b200_plane* planes, 
     plan.nfix = fix;
     plan.rec_stride = std::max(rec, 1);
     plan.pitch = ((BPS * S + O) + 3) & ~3;
+}
+
+// the mirror padding must stay inside the plane (cpu_source/getframe_impl.cpp:44-62 reads 2*ox - x)
+bool plane_fits(int width, int height, int B, int S) {
+    const int pw = dft2::pad_size(width, B, S), ph = dft2::pad_size(height, B, S);
+    const int ox = (pw - width) / 2, oy = (ph - height) / 2;
+    return width > std::max(ox, pw - width - ox) && height > std::max(oy, ph - height - oy);
+}
+
+int make_plan(const dfttest2_b200_filter* f, const dfttest2_b200_plane* planes, int n, int bps_bytes, Plan& plan) {
+    std::vector<PlaneRef> refs(n);
+    for (int i = 0; i < n; ++i) {
+        const dfttest2_b200_plane& p = planes[i];
+        if (!plane_fits(p.width, p.height, f->B, f->S))
+            return fail(DFTTEST2_B200_EINVAL, "plane too small for the block size");
+        for (int t = 0; t < f->T; ++t) {
+            if (p.src[t] == nullptr) return fail(DFTTEST2_B200_EINVAL, "null source plane");
+        }
+        if (!p.dst) return fail(DFTTEST2_B200_EINVAL, "null destination plane");
+        if (p.src_stride % bps_bytes || p.dst_stride % bps_bytes || p.src_stride < (ptrdiff_t)p.width * bps_bytes ||
+            p.dst_stride < (ptrdiff_t)p.width * bps_bytes)
+            return fail(DFTTEST2_B200_EINVAL, "invalid stride");
+        PlaneRef& r = refs[i];
+        std::memset(&r, 0, sizeof(r));
+        for (int t = 0; t < f->T; ++t) r.src[t] = p.src[t];
+        r.dst = p.dst;
+        r.src_stride = p.src_stride / bps_bytes;
+        r.dst_stride = p.dst_stride / bps_bytes;
+        r.width = p.width;
+        r.height = p.height;
+    }
+    plan_units(f->B, f->S, f->var.nw * f->var.bpw, refs, 4LL * f->num_sms, plan);
     return 0;
 }
 
@@ -336,21 +386,21 @@ int launch(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, floa
     a.njobs = (int)plan.jobs.size();
     a.nunits = plan.nunits;
     a.nfix = plan.nfix;
-    a.kind = kind;
-    a.scale = scale;
-    a.peak = peak;
+    a.p.kind = kind;
+    a.p.scale = scale;
+    a.p.peak = peak;
     a.block_step = f->S;
-    a.filter_type = f->filter_type;
-    a.sigma2 = f->sigma2;
-    a.pmin = f->pmin;
-    a.pmax = f->pmax;
-    a.g_div = f->zero_mean ? f->g_div : 0.0f;
-    a.win = f->d_win;
-    a.wsyn = f->d_wsyn;
-    a.sig = sig_override ? sig_override : f->d_sig;
-    a.sig2 = sig_override ? sig2_override : (f->asym ? f->d_sig2 : nullptr);
-    a.wfe = f->d_wfe;
-    a.wmask = f->zero_mean ? f->wmask : 0;
+    a.p.filter_type = f->filter_type;
+    a.p.sigma2 = f->sigma2;
+    a.p.pmin = f->pmin;
+    a.p.pmax = f->pmax;
+    a.p.g_div = f->zero_mean ? f->g_div : 0.0f;
+    a.p.win = f->d_win;
+    a.p.wsyn = f->d_wsyn;
+    a.p.sig = sig_override ? sig_override : f->d_sig;
+    a.p.sig2 = sig_override ? sig2_override : (f->asym ? f->d_sig2 : nullptr);
+    a.p.wfe = f->d_wfe;
+    a.p.wmask = f->zero_mean ? f->wmask : 0;
     a.scratch = slot.d_scratch;
     a.rec_stride = plan.rec_stride;
     a.ring_pitch = plan.pitch;
@@ -1157,21 +1207,21 @@ extern "C" int dfttest2_b200_process_plane_noalloc(const dfttest2_b200_params* p
     a.njobs = 1;
     a.nunits = nsx * nsy;
     a.nfix = (nsx - 1) * O * plane->height + (nsy - 1) * O * plane->width;
-    a.kind = kind;
-    a.scale = scale;
-    a.peak = peak;
+    a.p.kind = kind;
+    a.p.scale = scale;
+    a.p.peak = peak;
     a.block_step = S;
-    a.filter_type = p->filter_type;
-    a.sigma2 = (float)p->sigma2;
-    a.pmin = (float)p->pmin;
-    a.pmax = (float)p->pmax;
-    a.g_div = g_div;
-    a.win = reinterpret_cast<const float*>(base + off_win);
-    a.wsyn = reinterpret_cast<const float*>(base + off_wsyn);
-    a.sig = reinterpret_cast<const float*>(base + off_sig);
-    a.sig2 = asym ? reinterpret_cast<const float*>(base + off_sig2) : nullptr;
-    a.wfe = reinterpret_cast<const float*>(base + off_wfe);
-    a.wmask = zero_mean ? wmask : 0;
+    a.p.filter_type = p->filter_type;
+    a.p.sigma2 = (float)p->sigma2;
+    a.p.pmin = (float)p->pmin;
+    a.p.pmax = (float)p->pmax;
+    a.p.g_div = g_div;
+    a.p.win = reinterpret_cast<const float*>(base + off_win);
+    a.p.wsyn = reinterpret_cast<const float*>(base + off_wsyn);
+    a.p.sig = reinterpret_cast<const float*>(base + off_sig);
+    a.p.sig2 = asym ? reinterpret_cast<const float*>(base + off_sig2) : nullptr;
+    a.p.wfe = reinterpret_cast<const float*>(base + off_wfe);
+    a.p.wmask = zero_mean ? wmask : 0;
     a.scratch = reinterpret_cast<float*>(base + off_band);
     a.rec_stride = rec;
     a.ring_pitch = ((BPS * S + O) + 3) & ~3;
@@ -1190,3 +1240,5 @@ extern "C" int dfttest2_b200_process_plane_noalloc(const dfttest2_b200_params* p
     }
     return 0;
 }
+
+#include "dfttest_batch.cuh"

@@ -56,6 +56,25 @@ struct PlaneJob {
     int nsx, nsy;         // unit split of the block grid
     int unit_base;        // first global unit id of this job
     int fix_base;         // first global fix-up pixel id of this job
+    int param;            // index into KernelArgs::params (batched launches)
+    int pad_;
+};
+
+// sample format and filter of a plane: launch-wide, or per job in a batch
+struct FilterParams {
+    int kind;          // SampleKind
+    float scale;       // 2^-(bits-8) for integers, 255 for float
+    float peak;        // 2^bits - 1
+    int filter_type;   // 0..6
+    float sigma2, pmin, pmax;
+    float g_div;       // Re(window_freq[0,0,0]); 0 disables zero-mean
+    int wmask;         // bit p set when temporal plane p of the window spectrum is not identically zero
+    int pad_;
+    const float* win;  // [T][B][B] analysis window
+    const float* wsyn; // [B][B] synthesis window
+    const float* sig;  // [T][B/2+2][B] sigma per gain slot and column lane
+    const float* sig2; // [T][B/2+2][B] partner sigma (packed lanes, asymmetric sigma), may be null
+    const float* wfe;  // [T][B/2+2][B][2] window spectrum per gain slot (zero-mean)
 };
 
 struct KernelArgs {
@@ -63,19 +82,9 @@ struct KernelArgs {
     int njobs;
     int nunits;
     int nfix;
-    int kind;          // SampleKind
-    float scale;       // 2^-(bits-8) for integers, 255 for float
-    float peak;        // 2^bits - 1
     int block_step;    // S
-    int filter_type;   // 0..6
-    float sigma2, pmin, pmax;
-    float g_div;       // Re(window_freq[0,0,0]); 0 disables zero-mean
-    const float* win;  // [T][B][B] analysis window * scale
-    const float* wsyn; // [B][B] synthesis window
-    const float* sig;  // [T][B/2+2][B] sigma per gain slot and column lane
-    const float* sig2; // [T][B/2+2][B] partner sigma (packed lanes, asymmetric sigma), may be null
-    const float* wfe;  // [T][B/2+2][B][2] window spectrum per gain slot (zero-mean)
-    int wmask;         // bit p set when temporal plane p of the window spectrum is not identically zero
+    FilterParams p;    // every job's format and filter, unless params is set
+    const FilterParams* params;  // per-job formats and filters (PlaneJob::param), may be null
     float* scratch;    // per-unit band records
     int rec_stride;    // floats per unit record
     int ring_pitch;    // floats per ring row
@@ -174,7 +183,7 @@ __device__ __forceinline__ float rcp_approx(float x) {
 // FT 0 is the Wiener gain max((psd - s) / (psd + 1e-15), 0), evaluated as
 // max(1 - s * rcp(psd + 1e-15), 0); the other types keep IEEE division.
 template <int FT>
-__device__ __forceinline__ float gain(float psd, float s, const KernelArgs& a) {
+__device__ __forceinline__ float gain(float psd, float s, const FilterParams& a) {
     if constexpr (FT == 0) {
         return fmaxf(fmaf(-s, rcp_approx(psd + 1e-15f), 1.0f), 0.0f);
     } else if constexpr (FT == 1) {
@@ -192,7 +201,7 @@ __device__ __forceinline__ float gain(float psd, float s, const KernelArgs& a) {
     }
 }
 
-__device__ __forceinline__ float gain_rt(int ft, float psd, float s, const KernelArgs& a) {
+__device__ __forceinline__ float gain_rt(int ft, float psd, float s, const FilterParams& a) {
     switch (ft) {
     case 0: return fmaxf(__fdiv_rn(psd - s, psd + 1e-15f), 0.0f);
     case 1: return gain<1>(psd, s, a);
@@ -214,7 +223,7 @@ constexpr int kFilterGeneric = 7;
 // ZM = false: the plane's window spectrum is zero, so the zero-mean terms vanish
 template <int FC, bool ZM = true>
 __device__ __forceinline__ void apply_bin(float& re, float& im, float s, float s2, bool dual, float2 w, float g,
-                                          const KernelArgs& a) {
+                                          const FilterParams& a) {
     const float dre = ZM ? fmaf(-g, w.x, re) : re;
     const float dim = ZM ? fmaf(-g, w.y, im) : im;
     const float psd = fmaf(dim, dim, dre * dre);
@@ -392,7 +401,7 @@ template <int M> __device__ __forceinline__ void half_dft_inv(float (&re)[M], fl
 template <int M, int B, int FC, bool ZM>
 __device__ __forceinline__ void gain_lane_zm(float (&re)[M], float (&im)[M], const float* __restrict__ sig,
                                              const float* __restrict__ sig2, const float* __restrict__ wfe, int w,
-                                             float g, bool dual, const KernelArgs& a) {
+                                             float g, bool dual, const FilterParams& a) {
 #pragma unroll
     for (int j = 0; j < M; ++j) {
         const float s = sig[j * B + w];
@@ -405,7 +414,7 @@ __device__ __forceinline__ void gain_lane_zm(float (&re)[M], float (&im)[M], con
 template <int M, int B, int FC>
 __device__ __forceinline__ void gain_lane(float (&re)[M], float (&im)[M], const float* __restrict__ sig,
                                           const float* __restrict__ sig2, const float* __restrict__ wfe, int w, float g,
-                                          bool dual, bool has_w, const KernelArgs& a) {
+                                          bool dual, bool has_w, const FilterParams& a) {
     if (has_w)
         gain_lane_zm<M, B, FC, true>(re, im, sig, sig2, wfe, w, g, dual, a);
     else
@@ -458,7 +467,7 @@ __device__ __forceinline__ void for_pairs(int h, F&& f) {
 template <int B, int T, int FC>
 __device__ __forceinline__ void column_task(float* __restrict__ wb, float g, const float* __restrict__ sm_sig,
                                             const float* __restrict__ sm_sig2, const float* __restrict__ sm_wfe, int w,
-                                            bool dual_tables, bool store, const KernelArgs& a) {
+                                            bool dual_tables, bool store, const FilterParams& a) {
     using TL = Tile<B>;
     constexpr int M = B / 2;
     constexpr int R = (T - 1) / 2;
@@ -652,10 +661,18 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
     }
     // the plane descriptor is read many times per step: keep it on chip
     __shared__ PlaneJob s_job;
+    // and so are its format and filter
+    __shared__ FilterParams s_par;
+    static_assert(sizeof(PlaneJob) / sizeof(int) <= 32 && sizeof(FilterParams) / sizeof(int) <= 32, "descriptor size");
     if (tid < (int)(sizeof(PlaneJob) / sizeof(int)))
         reinterpret_cast<int*>(&s_job)[tid] = reinterpret_cast<const int*>(&a.jobs[lo])[tid];
+    if (tid >= 32 && tid < 32 + (int)(sizeof(FilterParams) / sizeof(int))) {
+        const FilterParams* src = a.params ? a.params + a.jobs[lo].param : &a.p;
+        reinterpret_cast<int*>(&s_par)[tid - 32] = reinterpret_cast<const int*>(src)[tid - 32];
+    }
     __syncthreads();
     const PlaneJob& job = s_job;
+    const FilterParams& P = s_par;
     const int W = job.width, Hh = job.height;
     const int pw = pad_size(W, B, S), ph = pad_size(Hh, B, S);
     const int pnx = (pw - B) / S + 1, pny = (ph - B) / S + 1;
@@ -669,8 +686,8 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
         return;
     }
     float* rec = a.scratch + (size_t)uid * a.rec_stride;
-    const bool is_float = (a.kind == kF32);
-    const float inv_scale = 1.0f / a.scale;  // exact for the power-of-two integer scales
+    const bool is_float = (P.kind == kF32);
+    const float inv_scale = 1.0f / P.scale;  // exact for the power-of-two integer scales
 
     // --- constants into shared memory -----------------------------------
     float* s_win = sm + L::o_win;
@@ -683,14 +700,14 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
     float* s_in = sm + L::o_ring;
     float* s_ola = s_in + L::in_ring_floats(pitch);
     // scale * window, rounded once as in load_block (cpu_source/getframe_impl.cpp:137)
-    for (int i = tid; i < T * B * B; i += NT) s_win[(i / B) * TL::WP + (i % B)] = a.scale * a.win[i];
-    for (int i = tid; i < B * B; i += NT) s_wsyn[(i / B) * TL::WP + (i % B)] = a.wsyn[i];
-    const bool dual_tables = (FC != kFilterWiener) && a.sig2 != nullptr;
+    for (int i = tid; i < T * B * B; i += NT) s_win[(i / B) * TL::WP + (i % B)] = P.scale * P.win[i];
+    for (int i = tid; i < B * B; i += NT) s_wsyn[(i / B) * TL::WP + (i % B)] = P.wsyn[i];
+    const bool dual_tables = (FC != kFilterWiener) && P.sig2 != nullptr;
     for (int i = tid; i < T * L::NSLOT * B; i += NT) {
-        s_sig[i] = a.sig[i];
-        if (dual_tables) s_sig2[i] = a.sig2[i];
+        s_sig[i] = P.sig[i];
+        if (dual_tables) s_sig2[i] = P.sig2[i];
     }
-    for (int i = tid; i < 2 * T * L::NSLOT * B; i += NT) s_wfe[i] = a.wfe[i];
+    for (int i = tid; i < 2 * T * L::NSLOT * B; i += NT) s_wfe[i] = P.wfe[i];
     for (int i = tid; i < L::ola_floats(pitch); i += NT) s_ola[i] = 0.0f;
 
     const int fw = u.fw;
@@ -702,7 +719,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
 
     // input rows [r_lo, r_lo + nr) of every temporal plane: element i of the
     // flattened (t, row, x) range -> (plane, ring offset, global index)
-    const int esz = a.kind == kF32 ? 4 : (a.kind == kU16 ? 2 : 1);
+    const int esz = P.kind == kF32 ? 4 : (P.kind == kU16 ? 2 : 1);
     auto stage_item = [&](int i, int r_lo, int nr, float inv_nr_rl, float inv_rl, int& t, int& soff, long long& gidx) {
         t = div_small(i, inv_nr_rl);
         const int rem = i - t * nr * rowlen;
@@ -722,7 +739,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
             int t, soff;
             long long gidx;
             stage_item(i, u.by0 * S, nr, inv_nr_rl, inv_rl, t, soff, gidx);
-            s_in[soff] = load_sample(job.src[t], gidx, a.kind);
+            s_in[soff] = load_sample(job.src[t], gidx, P.kind);
         }
     }
 
@@ -743,9 +760,9 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
             const float dc = row_task<B, T>(wbl, s_in, pitch, (by * S + lw) % B, blr * S, s_win, lw, vec, valid);
             const float tot = block_row_sum<B>(dc);
             // g = DC / Re(WF[0]) (cpu_source/kernel.hpp:1945)
-            if (lw == 0 && valid) s_g[bl] = a.g_div != 0.0f ? __fdiv_rn(tot, a.g_div) : 0.0f;
+            if (lw == 0 && valid) s_g[bl] = P.g_div != 0.0f ? __fdiv_rn(tot, P.g_div) : 0.0f;
             __syncwarp();
-            column_task<B, T, FC>(wbl, s_g[bl], s_sig, s_sig2, s_wfe, lw, dual_tables, valid, a);
+            column_task<B, T, FC>(wbl, s_g[bl], s_sig, s_sig2, s_wfe, lw, dual_tables, valid, P);
             __syncwarp();
             if (valid) inverse_row_task<B>(wbl, s_wsyn, lw);
         }
@@ -766,7 +783,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
                 int t;
                 long long gidx;
                 stage_item(i, n_lo, S, inv_nr_rl, inv_rl, t, pf_off[k], gidx);
-                pf[k] = load_raw(job.src[t], gidx, a.kind);
+                pf[k] = load_raw(job.src[t], gidx, P.kind);
             }
         }
 
@@ -777,7 +794,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
             const int px = x0 + lx;
             if (px < ox || px >= ox + W || py < oy || py >= oy + Hh) return;
             if (px >= excl_x0 && px < excl_x1 && py >= excl_y0 && py < excl_y1) {
-                store_sample(job.dst, (long long)(py - oy) * job.dst_stride + (px - ox), v, a.kind, a.scale, a.peak,
+                store_sample(job.dst, (long long)(py - oy) * job.dst_stride + (px - ox), v, P.kind, P.scale, P.peak,
                              is_float ? 0.0f : inv_scale);
             } else {
                 rec[band_index(lx, py - u.by0 * S, fw, u.fh, O)] = v;
@@ -829,12 +846,12 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
         // ---- store the prefetched rows (and any beyond the register budget)
 #pragma unroll
         for (int k = 0; k < PF; ++k)
-            if (pf_off[k] >= 0) s_in[pf_off[k]] = raw_to_float(pf[k], a.kind);
+            if (pf_off[k] >= 0) s_in[pf_off[k]] = raw_to_float(pf[k], P.kind);
         for (int i = tid + PF * NT; i < n_items; i += NT) {
             int t, soff;
             long long gidx;
             stage_item(i, n_lo, S, inv_nr_rl, inv_rl, t, soff, gidx);
-            s_in[soff] = load_sample(job.src[t], gidx, a.kind);
+            s_in[soff] = load_sample(job.src[t], gidx, P.kind);
         }
         // warm L2 with the rows of the step after next (one request per 128 B)
         if (by + 2 < u.by1) {
@@ -881,6 +898,7 @@ __global__ void __launch_bounds__(256) dfttest_fixup_kernel(const __grid_constan
             if (a.jobs[mid].fix_base <= gid) lo = mid; else hi = mid - 1;
         }
         const PlaneJob& job = a.jobs[lo];
+        const FilterParams& P = a.params ? a.params[job.param] : a.p;
         const int W = job.width, Hh = job.height;
         const int pw = pad_size(W, B, S), ph = pad_size(Hh, B, S);
         const int pnx = (pw - B) / S + 1, pny = (ph - B) / S + 1;
@@ -915,7 +933,7 @@ __global__ void __launch_bounds__(256) dfttest_fixup_kernel(const __grid_constan
                 acc += a.scratch[(size_t)uid * a.rec_stride + band_index(px - u.bx0 * S, py - u.by0 * S, u.fw, u.fh, O)];
             }
         }
-        store_sample(job.dst, (long long)(py - oy) * job.dst_stride + (px - ox), acc, a.kind, a.scale, a.peak);
+        store_sample(job.dst, (long long)(py - oy) * job.dst_stride + (px - ox), acc, P.kind, P.scale, P.peak);
     }
 }
 

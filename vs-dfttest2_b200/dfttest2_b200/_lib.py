@@ -69,6 +69,27 @@ class GradPlane(ctypes.Structure):
     ]
 
 
+class Clip(ctypes.Structure):
+    """dfttest2_b200_clip: one device-resident clip of a multi-clip batch."""
+
+    _fields_ = [
+        ("filter", c_void_p),
+        ("src", c_void_p),
+        ("src_stride", c_ssize_t),
+        ("src_frame_bytes", c_ssize_t),
+        ("dst", c_void_p),
+        ("dst_stride", c_ssize_t),
+        ("dst_frame_bytes", c_ssize_t),
+        ("nframes", c_int),
+        ("width", c_int),
+        ("height", c_int),
+        ("sample_type", c_int),
+        ("bits_per_sample", c_int),
+    ]
+
+
+BATCH_TUNE = 1
+
 # every symbol include/dfttest2_b200.h declares, with its ctypes signature
 SIGNATURES = {
     "dfttest2_b200_params_init": (None, [POINTER(Params)]),
@@ -82,6 +103,10 @@ SIGNATURES = {
     ),
     "dfttest2_b200_process_planes_sigma": (c_int, [c_void_p, POINTER(Plane), c_int, c_int, c_int, c_void_p, c_void_p]),
     "dfttest2_b200_backward_planes": (c_int, [c_void_p, POINTER(GradPlane), c_int, c_void_p, c_void_p, c_void_p]),
+    "dfttest2_b200_batch_create": (c_int, [POINTER(Clip), c_int, c_int, POINTER(c_void_p)]),
+    "dfttest2_b200_batch_run": (c_int, [c_void_p, c_void_p]),
+    "dfttest2_b200_batch_describe": (c_int, [c_void_p, ctypes.c_char_p, c_int]),
+    "dfttest2_b200_batch_free": (None, [c_void_p]),
     "dfttest2_b200_process_plane_noalloc": (c_int, [POINTER(Params), POINTER(Plane), c_int, c_int, c_void_p]),
     "dfttest2_b200_rdft": (c_int, [POINTER(c_double), c_int, POINTER(c_int), c_int, POINTER(c_double), c_int]),
     "dfttest2_b200_version": (c_char_p, []),

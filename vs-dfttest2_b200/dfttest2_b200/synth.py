@@ -56,3 +56,62 @@ def make_clip(fmt: VideoFormat, width: int, height: int, frames: int, seed: int,
             noisy.append(np.round(np.clip(v, 0, 1) * peak).astype(fmt.dtype))
             clean.append(np.round(np.clip(c, 0, 1) * peak).astype(fmt.dtype))
     return Clip(noisy, fmt), Clip(clean, fmt)
+
+
+def make_clip_device(fmt: VideoFormat, width: int, height: int, frames: int, seed: int, noise_sigma: float,
+                     device="cuda") -> list:
+    """The same generator evaluated by torch on the device (float32 phases),
+    for workloads too large to build on the host.  Returns the noisy planes
+    as (N, H, W) CUDA tensors of the format's sample type."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    planes = []
+    for p in range(fmt.num_planes):
+        pw, ph = plane_dims(fmt, width, height, p)
+        k = 16
+        fx, fy, a, dx, dy = (torch.tensor(rng.uniform(lo, hi, k), dtype=torch.float32, device=device)
+                             for lo, hi in ((0, 0.25), (0, 0.25), (0, 0.1), (-1, 1), (-1, 1)))
+        phi = torch.tensor(rng.uniform(0, 2 * np.pi, k), dtype=torch.float32, device=device)
+        xs = torch.arange(pw, dtype=torch.float32, device=device)
+        ys = torch.arange(ph, dtype=torch.float32, device=device)
+        ts = torch.arange(frames, dtype=torch.float32, device=device)
+        ax = 2 * np.pi * torch.outer(xs, fx)                                      # (w, k)
+        right = torch.cat([torch.cos(ax), torch.sin(ax)], dim=1).T                # (2k, w)
+        ay = (2 * np.pi * torch.outer(ys, fy))[None] + (phi - 2 * np.pi * torch.outer(ts, fx * dx + fy * dy))[:, None]
+        left = torch.cat([torch.sin(ay) * a, torch.cos(ay) * a], dim=2)           # (n, h, 2k)
+        v = 0.5 + left @ right
+        v += torch.randn(v.shape, generator=gen, device=device) * noise_sigma
+        if fmt.sample_type == FLOAT:
+            planes.append(v.contiguous())
+        else:
+            peak = (1 << fmt.bits_per_sample) - 1
+            q = torch.round(torch.clamp(v, 0, 1) * peak)
+            if fmt.bits_per_sample <= 8:
+                planes.append(q.to(torch.uint8).contiguous())
+            else:  # 16-bit samples travel as int16 tensors holding the unsigned bit pattern
+                qi = q.to(torch.int32)
+                planes.append(torch.where(qi >= 32768, qi - 65536, qi).to(torch.int16).contiguous())
+    return planes
+
+
+def batch_specs(seed: int = 0, nclips: int = 32) -> list[dict]:
+    """Clips of the multi-clip batching workload: resolution from {640x360,
+    1280x720, 1920x1080, 3840x2160}, 4..32 frames, GRAYS / YUV420P8 /
+    YUV420P16, sbsize in {8, 16, 32} with sosize = 3/4 sbsize, tbsize in
+    {1, 3, 5}, ftype in {0, 1}, flat sigma ~ U[2, 16]."""
+    from .clip import GRAYS, YUV420P8, YUV420P16
+
+    rng = np.random.default_rng(seed)
+    res = [(640, 360), (1280, 720), (1920, 1080), (3840, 2160)]
+    fmts = [GRAYS, YUV420P8, YUV420P16]
+    out = []
+    for i in range(nclips):
+        w, h = res[int(rng.integers(4))]
+        sb = int(rng.choice([8, 16, 32]))
+        out.append(dict(width=w, height=h, frames=int(rng.integers(4, 33)), fmt=fmts[int(rng.integers(3))], sbsize=sb,
+                        sosize=sb * 3 // 4, tbsize=int(rng.choice([1, 3, 5])), ftype=int(rng.integers(2)),
+                        sigma=float(rng.uniform(2, 16)), seed=seed * 1000 + i))
+    return out
