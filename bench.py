@@ -43,6 +43,9 @@ W, H = 1920, 1080
 SLOCATION = [0.0, 12.0, 1 / 3, 28 / 3, 2 / 3, 20 / 3, 1.0, 4.0]
 FLOP_PER_BLOCK = {1: 9473, 3: 26385, 5: 47329, 7: 74033}  # B = 16, reference codelet counts
 METRIC = "1080p YUV420P16 frames/s (DFTTest sbsize16 sosize12 tbsize3, all planes)"
+# DRAM bytes (read + write) of the unit kernel per 1080p YUV420P16 frame, from one ncu capture of a
+# 24-frame launch (profiles/dfttest_unit_16x3_yuv420p16.md); traffic grows with the frames processed
+DRAM_BYTES_PER_FRAME = 17_790_347
 
 
 def workload_args():
@@ -490,7 +493,9 @@ def main():
                 "d2h_bytes_per_step": bytes_in, "path": "dfttest2_b200_process_clip_host, pinned host memory"},
         "gpu_launches": 2 * opts.steps,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                     "traffic": None,
+                     "traffic": DRAM_BYTES_PER_FRAME * (hi - lo),
+                     "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum per launch, scaled from a 24-frame "
+                                     "ncu capture (profiles/dfttest_unit_16x3_yuv420p16.md)",
                      "peak_source": "cuBLAS FP32 SGEMM (TF32 off) measured in this run; nominal 148 SM x 128 x 2 x "
                                     "1.965 GHz = 74.4",
                      "flop_per_step": flops_step, "hbm_algorithmic_gbs": algo_bytes / (ms_per_step * 1e-3) / 1e9,
