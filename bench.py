@@ -365,6 +365,8 @@ def main():
     ap.add_argument("--workload", default="yuv1080p", choices=["yuv1080p", "batch"],
                     help="batch: the 32-clip multi-clip batching workload (one GPU)")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--tc-steps", type=int, default=10,
+                    help="steps timed for each tensor-core precision mode (0 skips the comparison)")
     opts = ap.parse_args()
     if opts.workload == "batch":
         if opts.impl == "reference":
@@ -448,6 +450,33 @@ def main():
     value = frames_done / (ms * 1e-3)
     ms_per_step = ms / opts.steps
 
+    # ---- tensor-core form of the transforms on the same workload, against the plain FP32 output
+    tc_results = {}
+    if opts.tc_steps > 0:
+        plain_out = [o.clone() for o in dev_out]
+        for mode in ("tc_bf16x3", "tc_tf32"):
+            flt.set_precision(mode)
+            for _ in range(2):
+                step()
+            torch.cuda.synchronize()
+            t_start, t_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t_start.record(stream)
+            for _ in range(opts.tc_steps):
+                step()
+            t_stop.record(stream)
+            torch.cuda.synchronize()
+            ms_tc = max_over_ranks(t_start.elapsed_time(t_stop), pg) / opts.tc_steps
+            worst, exact, total = 0, 0, 0
+            for a_, b_ in zip(dev_out, plain_out):
+                d = ((a_.to(torch.int32) & 0xFFFF) - (b_.to(torch.int32) & 0xFFFF)).abs()
+                worst = max(worst, int(d.max().item()))
+                exact += int((d == 0).sum().item())
+                total += d.numel()
+            tc_results[mode] = {"value": world * (hi - lo) / (ms_tc * 1e-3), "unit": "frames/s", "ms_per_step": ms_tc,
+                                "speedup_vs_fp32": ms_per_step / ms_tc, "max_lsb_vs_fp32": worst,
+                                "exact_vs_fp32": exact / max(total, 1), "steps": opts.tc_steps}
+        flt.set_precision("fp32")
+
     # ---- end to end through the C ABI host path (pinned host buffers)
     pinned_in = [torch.from_numpy(p.view(np.int16)).pin_memory() for p in host_planes]
     pinned_out = [torch.empty((in_hi - in_lo,) + tuple(p.shape[1:]), dtype=torch.int16).pin_memory()
@@ -501,6 +530,7 @@ def main():
                      "flop_per_step": flops_step, "hbm_algorithmic_gbs": algo_bytes / (ms_per_step * 1e-3) / 1e9,
                      "hbm_peak_gbs": measured_peaks().get("hbm_gbs")},
         "clocks": clocks.summary(),
+        "tc": tc_results,
     }
     if world == 1 and rank == 0 and not opts.no_cpu_baseline:
         result["cpu_baseline"] = cpu_reference_fps(args, host_planes)

@@ -153,6 +153,23 @@ int dfttest2_b200_process_planes_sigma(dfttest2_b200_filter* f, const dfttest2_b
 int dfttest2_b200_backward_planes(dfttest2_b200_filter* f, const dfttest2_b200_grad_plane* planes, int nplanes,
                                   const float* sigma, float* grad_sigma, void* stream);
 
+/* Arithmetic of the per-block transforms.  FP32 (the default) runs them as
+ * FP32 FFT codelets on the CUDA cores, like the reference's kernels
+ * (nvrtc_source/kernels.cu:86-295).  The TC modes run them as dense products
+ * on the tensor cores (tcgen05.mma, FP32 accumulation): TC_BF16X3 splits
+ * every operand into bf16 hi + lo and sums three products (about 16
+ * significant bits), TC_TF32 and TC_BF16 use one product (10 and 7 bits).
+ * Available for block_size 16 with radius 0 or 1 and block_size 32 with
+ * radius 0; the gain, zero-mean and overlap-add stay in FP32.  No
+ * counterpart in the reference.  Applies to the process_* paths of the
+ * filter (not to the differentiable and batch paths, which stay FP32). */
+#define DFTTEST2_B200_FP32 0
+#define DFTTEST2_B200_TC_BF16X3 1
+#define DFTTEST2_B200_TC_TF32 2
+#define DFTTEST2_B200_TC_BF16 3
+
+int dfttest2_b200_set_precision(dfttest2_b200_filter* f, int mode);
+
 /* Multi-clip batches.  The reference filters one clip per filter instance,
  * one frame per DFTTestGetFrame call (nvrtc_source/source.cpp:356-605); a
  * batch filters many device-resident clips, each with its own DFTTest

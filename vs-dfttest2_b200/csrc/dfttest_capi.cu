@@ -28,6 +28,7 @@
 #include "dfttest2_b200.h"
 #include "dfttest_kernel.cuh"
 #include "dfttest_adjoint.cuh"
+#include "dfttest_tc.cuh"
 
 #ifndef DFTTEST2_B200_VERSION
 #define DFTTEST2_B200_VERSION "0.1.0"
@@ -156,6 +157,10 @@ struct Slot {
     size_t sigtab_cap = 0;
     dft2::GradJob* d_gjobs = nullptr;
     size_t gjobs_cap = 0;
+    dft2::TcJob* d_tcjobs = nullptr;      // tensor-core form: work-list and accumulator planes
+    size_t tcjobs_cap = 0;
+    float* d_acc = nullptr;
+    size_t acc_cap = 0;
 };
 
 }  // namespace
@@ -184,6 +189,10 @@ struct dfttest2_b200_filter {
     int* d_sig_idx = nullptr;       // [T][B/2+2][B]
     int* d_sig2_idx = nullptr;
     int n_slots = 0;
+    // tensor-core form (dfttest2_b200_set_precision)
+    int tc_mode = 0;
+    void* d_gmat = nullptr;
+    int gmat_bytes = 0;
 
     std::vector<Slot> slots;
     std::vector<int> free_slots;
@@ -371,9 +380,182 @@ int make_plan(const dfttest2_b200_filter* f, const dfttest2_b200_plane* planes, 
     return 0;
 }
 
+// ---- tensor-core form ------------------------------------------------------
+using TcKernelFn = void (*)(const dft2::TcArgs);
+
+struct TcVariant {
+    TcKernelFn wiener = nullptr, generic = nullptr;
+    size_t (*smem)(int patch_w) = nullptr;
+    int gbytes = 0;
+    int tb = 0;  // blocks per tile
+    void (*build)(std::vector<char>&) = nullptr;
+};
+
+// the constant operands (N x K, K-major canonical layout) of the four products
+template <int B, int T, int MODE>
+void build_gmat(std::vector<char>& img) {
+    using L = dft2::TcLayout<B, T, MODE>;
+    constexpr int ESZ = L::ESZ;
+    img.assign(L::GBYTES, 0);
+    const double pi = 3.14159265358979323846;
+    auto put = [&](int off, int n, int k, int KT, double v) {
+        const int idx = off + dft2::op_index<ESZ>(n, k, KT);
+        if (MODE == dft2::kTcTf32) {
+            const float f = (float)v;
+            std::memcpy(&img[(size_t)idx * 4], &f, 4);
+        } else {
+            const __nv_bfloat16 h = __float2bfloat16_rn((float)v);
+            std::memcpy(&img[(size_t)idx * 2], &h, 2);
+            if (MODE == dft2::kTcBf16x3) {
+                const __nv_bfloat16 l = __float2bfloat16_rn((float)(v - (double)__bfloat162float(h)));
+                std::memcpy(&img[(size_t)(L::GELEM + idx) * 2], &l, 2);
+            }
+        }
+    };
+    // G1: packed r2c of a row, [j][x]
+    for (int j = 0; j < B; ++j)
+        for (int x = 0; x < B; ++x) {
+            const int k = j < 2 ? (j == 0 ? 0 : B / 2) : j / 2;
+            const double ang = 2.0 * pi * k * x / B;
+            put(L::g1, j, x, B, j < 2 ? std::cos(ang) : ((j & 1) ? -std::sin(ang) : std::cos(ang)));
+        }
+    // G2: F_t (x) F_y in real form, [(kt, c', ky)][(t, c, y)]
+    constexpr int K2 = L::K2;
+    for (int kt = 0; kt < T; ++kt)
+        for (int cp = 0; cp < 2; ++cp)
+            for (int ky = 0; ky < B; ++ky)
+                for (int t = 0; t < T; ++t)
+                    for (int c = 0; c < 2; ++c)
+                        for (int y = 0; y < B; ++y) {
+                            const double th = 2.0 * pi * ((double)(kt * t % T) / T + (double)(ky * y % B) / B);
+                            const double v = cp == c ? std::cos(th) : (c == 1 ? std::sin(th) : -std::sin(th));
+                            put(L::g2, (kt * 2 + cp) * B + ky, (t * 2 + c) * B + y, K2, v);
+                        }
+    // G4: inverse complex DFT over y, [(c', y)][(c, ky)]
+    for (int cp = 0; cp < 2; ++cp)
+        for (int y = 0; y < B; ++y)
+            for (int c = 0; c < 2; ++c)
+                for (int ky = 0; ky < B; ++ky) {
+                    const double ph = 2.0 * pi * (double)(ky * y % B) / B;
+                    const double v = cp == c ? std::cos(ph) : (c == 1 ? -std::sin(ph) : std::sin(ph));
+                    put(L::g4, cp * B + y, c * B + ky, 2 * B, v);
+                }
+    // G5: c2r of a packed row, [x][j]
+    for (int x = 0; x < B; ++x)
+        for (int j = 0; j < B; ++j) {
+            const int k = j < 2 ? (j == 0 ? 0 : B / 2) : j / 2;
+            const double ang = 2.0 * pi * (double)(k * x % B) / B;
+            put(L::g5, x, j, B, j < 2 ? std::cos(ang) : ((j & 1) ? -2.0 * std::sin(ang) : 2.0 * std::cos(ang)));
+        }
+}
+
+template <int B, int T, int MODE>
+TcVariant make_tc() {
+    TcVariant v;
+    v.wiener = dft2::dfttest_tc_kernel<B, T, MODE, dft2::kFilterWiener>;
+    v.generic = dft2::dfttest_tc_kernel<B, T, MODE, dft2::kFilterGeneric>;
+    v.smem = [](int pw) { return dft2::TcLayout<B, T, MODE>::bytes(pw); };
+    v.gbytes = dft2::TcLayout<B, T, MODE>::GBYTES;
+    v.tb = dft2::TcLayout<B, T, MODE>::TB;
+    v.build = build_gmat<B, T, MODE>;
+    return v;
+}
+
+template <int B, int T>
+TcVariant select_tc_mode(int mode) {
+    switch (mode) {
+    case dft2::kTcBf16x3: return make_tc<B, T, dft2::kTcBf16x3>();
+    case dft2::kTcTf32: return make_tc<B, T, dft2::kTcTf32>();
+    case dft2::kTcBf16: return make_tc<B, T, dft2::kTcBf16>();
+    }
+    return TcVariant{};
+}
+
+TcVariant select_tc(int B, int T, int mode) {
+    if (B == 16 && T == 1) return select_tc_mode<16, 1>(mode);
+    if (B == 16 && T == 3) return select_tc_mode<16, 3>(mode);
+#ifndef DFTTEST2_B200_ONLY_B16
+    if (B == 32 && T == 1) return select_tc_mode<32, 1>(mode);
+#endif
+    return TcVariant{};
+}
+
+int launch_tc(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, float scale, float peak,
+              cudaStream_t stream) {
+    const TcVariant v = select_tc(f->B, f->T, f->tc_mode);
+    if (!v.wiener) return fail(DFTTEST2_B200_EINVAL, "tensor-core form not available for these arguments");
+    const int B = f->B, S = f->S;
+    CUDA_TRY(cudaStreamWaitEvent(stream, slot.done, 0));
+    std::vector<dft2::TcJob> jobs(plan.jobs.size());
+    long long ntiles = 0;
+    size_t acc = 0;
+    for (size_t i = 0; i < plan.jobs.size(); ++i) {
+        const dft2::PlaneJob& p = plan.jobs[i];
+        dft2::TcJob& j = jobs[i];
+        std::memset(&j, 0, sizeof(j));
+        for (int t = 0; t < 7; ++t) j.src[t] = p.src[t];
+        j.dst = p.dst;
+        j.src_stride = p.src_stride;
+        j.dst_stride = p.dst_stride;
+        j.width = p.width;
+        j.height = p.height;
+        j.ntx = (dft2::pad_num(p.width, B, S) + v.tb - 1) / v.tb;
+        j.tile_base = (int)ntiles;
+        ntiles += (long long)j.ntx * dft2::pad_num(p.height, B, S);
+        if (ntiles > INT_MAX) return fail(DFTTEST2_B200_EINVAL, "too many planes in one call");
+        j.acc = reinterpret_cast<float*>(acc);  // offset for now
+        acc += (size_t)p.width * p.height;
+    }
+    if (jobs.size() > 65535) return fail(DFTTEST2_B200_EINVAL, "at most 65535 planes per call in the tensor-core form");
+    if (int rc = ensure(slot.d_tcjobs, slot.tcjobs_cap, jobs.size(), slot.done)) return rc;
+    if (int rc = ensure(slot.d_acc, slot.acc_cap, std::max<size_t>(acc, 1), slot.done)) return rc;
+    for (auto& j : jobs) j.acc = slot.d_acc + reinterpret_cast<size_t>(j.acc);
+    CUDA_TRY(cudaMemcpyAsync(slot.d_tcjobs, jobs.data(), jobs.size() * sizeof(dft2::TcJob), cudaMemcpyHostToDevice,
+                             stream));
+    CUDA_TRY(cudaMemsetAsync(slot.d_acc, 0, acc * sizeof(float), stream));
+    dft2::TcArgs a{};
+    a.jobs = slot.d_tcjobs;
+    a.njobs = (int)jobs.size();
+    a.ntiles = (int)ntiles;
+    a.block_step = S;
+    a.p.kind = kind;
+    a.p.scale = scale;
+    a.p.peak = peak;
+    a.p.filter_type = f->filter_type;
+    a.p.sigma2 = f->sigma2;
+    a.p.pmin = f->pmin;
+    a.p.pmax = f->pmax;
+    a.p.g_div = f->zero_mean ? f->g_div : 0.0f;
+    a.p.win = f->d_win;
+    a.p.wsyn = f->d_wsyn;
+    a.sigma = f->d_sigma_full;
+    a.wf = f->d_wf_full;
+    a.gmat = f->d_gmat;
+    a.gmat_bytes = f->gmat_bytes;
+    a.error_flag = slot.d_error;
+    const int patch_w = B + (v.tb - 1) * S;
+    const size_t smem = v.smem(patch_w);
+    if (smem > 227 * 1024) return fail(DFTTEST2_B200_EINVAL, "block step too large for the tensor-core form");
+    TcKernelFn kern = f->filter_type == 0 ? v.wiener : v.generic;
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
+    if (per_sm < 1) return fail(DFTTEST2_B200_ECUDA, "tensor-core kernel does not fit on an SM");
+    const int grid = std::max(1, std::min(a.ntiles, f->num_sms * std::min(per_sm, 2)));
+    kern<<<grid, 256, smem, stream>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    dim3 fg((unsigned)std::max<long long>(1, std::min<long long>(64, (acc / jobs.size() + 255) / 256)),
+            (unsigned)jobs.size());
+    dft2::dfttest_tc_finalize<<<fg, 256, 0, stream>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaEventRecord(slot.done, stream));
+    return 0;
+}
+
 int launch(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, float scale, float peak,
            cudaStream_t stream, const float* sig_override = nullptr, const float* sig2_override = nullptr) {
     if (plan.nunits == 0) return 0;
+    if (f->tc_mode && !sig_override) return launch_tc(f, slot, plan, kind, scale, peak, stream);
     CUDA_TRY(cudaStreamWaitEvent(stream, slot.done, 0));
     if (int rc = ensure(slot.d_jobs, slot.jobs_cap, plan.jobs.size(), slot.done)) return rc;
     const size_t scratch_need = (size_t)plan.nunits * plan.rec_stride;
@@ -501,6 +683,8 @@ void free_filter(dfttest2_b200_filter* f) {
         if (s.d_frames) cudaFree(s.d_frames);
         if (s.d_sigtab) cudaFree(s.d_sigtab);
         if (s.d_gjobs) cudaFree(s.d_gjobs);
+        if (s.d_tcjobs) cudaFree(s.d_tcjobs);
+        if (s.d_acc) cudaFree(s.d_acc);
         if (s.h_pinned) cudaFreeHost(s.h_pinned);
         if (s.stream) cudaStreamDestroy(s.stream);
         if (s.up) cudaStreamDestroy(s.up);
@@ -521,6 +705,7 @@ void free_filter(dfttest2_b200_filter* f) {
     cudaFree(f->d_wf_full);
     cudaFree(f->d_sig_idx);
     cudaFree(f->d_sig2_idx);
+    if (f->d_gmat) cudaFree(f->d_gmat);
     delete f;
 }
 
@@ -717,6 +902,33 @@ int dfttest2_b200_create(const dfttest2_b200_params* p, dfttest2_b200_filter** o
 }
 
 void dfttest2_b200_free(dfttest2_b200_filter* f) { free_filter(f); }
+
+int dfttest2_b200_set_precision(dfttest2_b200_filter* f, int mode) {
+    if (!f) return fail(DFTTEST2_B200_EINVAL, "null filter");
+    if (mode < DFTTEST2_B200_FP32 || mode > DFTTEST2_B200_TC_BF16)
+        return fail(DFTTEST2_B200_EINVAL, "unknown precision mode");
+    DeviceGuard dg(f->device);
+    // no launch of this filter may still read the old constants
+    for (Slot& s : f->slots)
+        if (s.done) CUDA_TRY(cudaEventSynchronize(s.done));
+    if (mode == DFTTEST2_B200_FP32) {
+        f->tc_mode = 0;
+        return 0;
+    }
+    const TcVariant v = select_tc(f->B, f->T, mode);
+    if (!v.wiener)
+        return fail(DFTTEST2_B200_EINVAL,
+                    "the tensor-core form supports block_size 16 with radius 0 or 1 and block_size 32 with radius 0");
+    std::vector<char> img;
+    v.build(img);
+    if (f->d_gmat) CUDA_TRY(cudaFree(f->d_gmat));
+    f->d_gmat = nullptr;
+    CUDA_TRY(cudaMalloc(&f->d_gmat, img.size()));
+    CUDA_TRY(cudaMemcpy(f->d_gmat, img.data(), img.size(), cudaMemcpyHostToDevice));
+    f->gmat_bytes = (int)img.size();
+    f->tc_mode = mode;
+    return 0;
+}
 
 int dfttest2_b200_process_planes(dfttest2_b200_filter* f, const dfttest2_b200_plane* planes, int nplanes,
                                  int sample_type, int bits_per_sample, void* stream) {

@@ -1,0 +1,531 @@
+// Tensor-core form of the DFTTest per-block pipeline: the transforms of
+// cpu_source/kernel.hpp:1899-1983 (fused) as dense products on the sm_100a
+// 5th-generation tensor cores (tcgen05.mma, operands in shared memory,
+// accumulators in tensor memory), with the elementwise work (operand
+// re-layout, hi/lo split, zero-mean, gain, temporal inverse of the centre
+// frame, synthesis window, overlap-add) on the CUDA cores.
+//
+// A tile is TB = 128 / B neighbouring blocks of one block row.  Per tile:
+//   G1  row r2c         rows (t, blk, y)  K = B (x)           N = B  (packed bins j)
+//   G2  col + temporal  rows (blk, kx)    K = (t, c, y) 2TB   N = (kt, c, ky) 2TB
+//       DFT (F_t (x) F_y in real form; kx padded to B rows, rows kx > B/2 unused)
+//   --  zero-mean, gain, inverse over t of the centre frame (CUDA cores)
+//   G4  inverse col DFT rows (blk, kx)    K = (c, ky) 2B      N = (c, y) 2B
+//   G5  c2r             rows (blk, y)     K = B (packed j)    N = B (x)
+// Packed bins j of a real row: j = 0 -> Re X0, 1 -> Re X_{B/2}, 2k -> Re Xk,
+// 2k + 1 -> Im Xk (k = 1 .. B/2 - 1); c2r ignores Im X0 and Im X_{B/2}.
+//
+// Precision modes: BF16X3 splits every operand into bf16 hi + lo and sums
+// hi*hi + hi*lo + lo*hi in FP32 (three MMAs per K step); BF16 and TF32 use
+// one MMA per K step.  Accumulation is FP32 in tensor memory.
+//
+// The overlap-add of a tile is summed in shared memory and added to a float
+// accumulator plane in global memory (atomic adds); a second kernel converts
+// the accumulators to the output format.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "dfttest_kernel.cuh"
+
+namespace dft2 {
+
+enum TcMode { kTcOff = 0, kTcBf16x3 = 1, kTcTf32 = 2, kTcBf16 = 3 };
+
+struct TcJob {
+    const void* src[7];
+    void* dst;
+    float* acc;             // accumulator plane, width x height floats (zeroed before the launch)
+    long long src_stride, dst_stride;  // elements
+    int width, height;
+    int tile_base;          // first global tile id
+    int ntx;                // tiles per block row
+};
+
+struct TcArgs {
+    const TcJob* jobs;
+    int njobs;
+    int ntiles;
+    int block_step;
+    FilterParams p;
+    const float* sigma;     // [T][B][X]
+    const float* wf;        // [T][B][X][2]
+    const void* gmat;       // the four constant operands, shared-memory image
+    int gmat_bytes;
+    int* error_flag;
+};
+
+// ---- PTX wrappers (tcgen05, mbarrier) --------------------------------------
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// shared-memory matrix descriptor: K-major, no swizzle (8-row x 16-byte core
+// matrices; lbo = byte step between core matrices along K, sbo = along M/N)
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version of sm_100
+    return d;                // base offset 0, swizzle none
+}
+
+// instruction descriptor of kind::f16 / kind::tf32: D f32, A and B K-major
+__host__ __device__ constexpr uint32_t idesc(int ab_format, int M, int N) {
+    return (1u << 4)                       // D format f32
+           | ((uint32_t)ab_format << 7)    // A format (1 = bf16, 2 = tf32)
+           | ((uint32_t)ab_format << 10)   // B format
+           | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+template <bool TF32>
+__device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
+    const uint32_t z = 0;
+    if constexpr (TF32) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n"
+            :: "r"(d_tmem), "l"(a), "l"(b), "r"(id), "r"(acc), "r"(z));
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n"
+            :: "r"(d_tmem), "l"(a), "l"(b), "r"(id), "r"(acc), "r"(z));
+    }
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+// bounded wait for the phase with the given parity; false when the limit ran out
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = smem_addr(bar);
+    for (int it = 0; it < (1 << 22); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done) : "r"(a), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void async_proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 8 consecutive 32-bit columns of this thread's lane
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmem_ld1(uint32_t taddr, float& v) {
+    uint32_t r;
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr));
+    v = __uint_as_float(r);
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// ---- operand layouts -------------------------------------------------------
+// element (m, k) of a K-major operand with KT columns, in elements of ESZ bytes
+template <int ESZ>
+__host__ __device__ constexpr int op_index(int m, int k, int KT) {
+    constexpr int PER = 16 / ESZ;  // elements per 16-byte core-matrix row
+    return (((m >> 3) * (KT / PER) + k / PER) * 8 + (m & 7)) * PER + (k % PER);
+}
+
+// operand store of one value: bf16 hi (+ lo) or tf32 (fp32 bits)
+template <int MODE>
+struct Operand {
+    static constexpr bool TF = MODE == kTcTf32;
+    static constexpr int ESZ = TF ? 4 : 2;
+    static constexpr bool SPLIT = MODE == kTcBf16x3;
+};
+
+// operand buffers hold a hi plane and (BF16X3) a lo plane `lo_off` bytes later
+template <int MODE>
+__device__ __forceinline__ void put(char* base, int lo_off, int idx, float v) {
+    if constexpr (MODE == kTcTf32) {
+        reinterpret_cast<float*>(base)[idx] = v;
+    } else {
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        reinterpret_cast<__nv_bfloat16*>(base)[idx] = h;
+        if constexpr (MODE == kTcBf16x3)
+            reinterpret_cast<__nv_bfloat16*>(base + lo_off)[idx] = __float2bfloat16_rn(v - __bfloat162float(h));
+    }
+}
+
+// 8 consecutive K values of one row (one 16-byte core-matrix row for bf16)
+template <int MODE>
+__device__ __forceinline__ void put8(char* base, int lo_off, int idx, const float (&v)[8]) {
+    if constexpr (MODE == kTcTf32) {
+        float4* p = reinterpret_cast<float4*>(reinterpret_cast<float*>(base) + idx);
+        // idx is a multiple of 4; the two halves lie in consecutive core matrices along K
+        p[0] = make_float4(v[0], v[1], v[2], v[3]);
+        reinterpret_cast<float4*>(reinterpret_cast<float*>(base) + idx + 32)[0] = make_float4(v[4], v[5], v[6], v[7]);
+    } else {
+        __align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            h[i] = __float2bfloat16_rn(v[i]);
+            l[i] = __float2bfloat16_rn(v[i] - __bfloat162float(h[i]));
+        }
+        *reinterpret_cast<uint4*>(reinterpret_cast<__nv_bfloat16*>(base) + idx) = *reinterpret_cast<const uint4*>(h);
+        if constexpr (MODE == kTcBf16x3)
+            *reinterpret_cast<uint4*>(reinterpret_cast<__nv_bfloat16*>(base + lo_off) + idx) =
+                *reinterpret_cast<const uint4*>(l);
+    }
+}
+
+// shared-memory plan of the tensor-core kernel (bytes)
+template <int B, int T, int MODE>
+struct TcLayout {
+    static constexpr int ESZ = Operand<MODE>::ESZ;
+    static constexpr int NPLANE = Operand<MODE>::SPLIT ? 2 : 1;
+    static constexpr int X = B / 2 + 1;
+    static constexpr int TB = 128 / B;       // blocks per tile
+    static constexpr int K2 = 2 * T * B;     // column + temporal stage width
+    // constant operands (N x K each), hi planes then lo planes
+    static constexpr int G1 = B * B, G2 = K2 * K2, G4 = 4 * B * B, G5 = B * B;
+    static constexpr int GELEM = G1 + G2 + G4 + G5;
+    static constexpr int g1 = 0, g2 = G1, g4 = G1 + G2, g5 = G1 + G2 + G4;  // element offsets in a plane
+    static constexpr int GBYTES = GELEM * ESZ * NPLANE;
+    // A operand region: the largest stage (A1 has T planes of 128 x B)
+    static constexpr int A1 = T * 128 * B, A2 = 128 * K2, A4 = 128 * 2 * B, A5 = 128 * B;
+    static constexpr int AELEM = A1 > A2 ? (A1 > A4 ? A1 : A4) : (A2 > A4 ? A2 : A4);
+    static constexpr int ABYTES = AELEM * ESZ * NPLANE;
+    static constexpr int o_g = 0;
+    static constexpr int o_a = (o_g + GBYTES + 127) & ~127;
+    static constexpr int o_tab = (o_a + ABYTES + 127) & ~127;  // floats from here
+    // float tables: scale * window [T][B][B], wsyn [B][B], sigma and WF as [kx][kt][ky]
+    static constexpr int F_WIN = 0, F_WSYN = T * B * B, F_SIG = F_WSYN + B * B, F_WF = F_SIG + X * T * B;
+    static constexpr int F_END = F_WF + 2 * X * T * B;
+    static constexpr int o_patch = o_tab + 4 * F_END;  // input rows [T][B][patch_w], then the overlap-add tile [B][patch_w]
+    static size_t bytes(int patch_w) { return (size_t)o_patch + 4 * (size_t)(T + 1) * B * patch_w + 64; }
+};
+
+template <int B, int T, int MODE, int FC>
+__global__ void __launch_bounds__(256, 2) dfttest_tc_kernel(const __grid_constant__ TcArgs a) {
+    using L = TcLayout<B, T, MODE>;
+    constexpr bool TF = MODE == kTcTf32;
+    constexpr int ESZ = L::ESZ;
+    constexpr int X = L::X, TB = L::TB, K2 = L::K2;
+    constexpr int R = (T - 1) / 2;
+    constexpr int NT = 256;
+    constexpr int KSTEP = TF ? 8 : 16;  // K per MMA
+    extern __shared__ __align__(128) char tc_smem[];
+    char* smem = tc_smem;
+    __shared__ uint64_t s_bar;
+    __shared__ uint32_t s_tmem;
+
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int row = ((warp & 3) << 5) | (tid & 31);  // tensor-memory lane of this thread
+    const int half = warp >> 2;                       // which half of the columns this thread handles
+    const int S = a.block_step;
+    const FilterParams& P = a.p;
+
+    char* g_hi = smem + L::o_g;
+    char* a_hi = smem + L::o_a;
+    constexpr int G_LO = L::GELEM * ESZ;  // lo plane offsets (BF16X3)
+    constexpr int A_LO = L::AELEM * ESZ;
+    float* tab = reinterpret_cast<float*>(smem + L::o_tab);
+    float* s_win = tab + L::F_WIN;
+    float* s_wsyn = tab + L::F_WSYN;
+    float* s_sig = tab + L::F_SIG;
+    float* s_wf = tab + L::F_WF;
+    const int PWID = B + (TB - 1) * S;                // patch width
+    float* s_patch = reinterpret_cast<float*>(smem + L::o_patch);
+    float* s_ola = s_patch + T * B * PWID;
+
+    // ---- one-time set-up: constants, tables, barrier, tensor memory
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(a.gmat);
+        uint4* dst = reinterpret_cast<uint4*>(g_hi);
+        for (int i = tid; i < a.gmat_bytes / 16; i += NT) dst[i] = src[i];
+    }
+    for (int i = tid; i < T * B * B; i += NT) s_win[i] = P.scale * P.win[i];
+    for (int i = tid; i < B * B; i += NT) s_wsyn[i] = P.wsyn[i];
+    for (int i = tid; i < X * T * B; i += NT) {
+        const int kx = i / (T * B), rem = i - kx * T * B;  // rem = kt * B + ky
+        const int src = rem * X + kx;                        // [kt][ky][kx]
+        s_sig[i] = a.sigma[src];
+        s_wf[2 * i] = P.g_div != 0.0f ? a.wf[2 * src] : 0.0f;
+        s_wf[2 * i + 1] = P.g_div != 0.0f ? a.wf[2 * src + 1] : 0.0f;
+    }
+    for (int i = tid; i < B * PWID; i += NT) s_ola[i] = 0.0f;
+    if (tid == 0) {
+        mbar_init(&s_bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_addr(&s_tmem)), "r"(256) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    async_proxy_fence();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+    constexpr uint32_t C_D1 = 0, C_D2 = 128, C_D4 = 0, C_D5 = 64;  // tensor-memory columns of the stages
+    uint32_t phase = 0;
+    bool s_fail_any = false;
+
+    // issue `nk` K steps of D(128 x N) = A(128 x K) * G(N x K)^T, commit, wait
+    auto gemm = [&](uint32_t d_col, int a_off, int a_kt, int g_off, int n, int nk) -> bool {
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t id = idesc(TF ? 2 : 1, 128, n);
+            const uint32_t a0 = smem_addr(a_hi) + a_off * ESZ, g0 = smem_addr(g_hi) + g_off * ESZ;
+            const uint32_t a_sbo = (a_kt * ESZ / 16) * 128, g_sbo = (a_kt * ESZ / 16) * 128;
+            for (int s = 0; s < nk; ++s) {
+                const uint32_t step = s * 256;  // two core matrices along K per MMA
+                const uint64_t ad = sdesc(a0 + step, 128, a_sbo), gd = sdesc(g0 + step, 128, g_sbo);
+                mma<TF>(tmem + d_col, ad, gd, id, s > 0 ? 1u : 0u);
+                if constexpr (MODE == kTcBf16x3) {
+                    mma<TF>(tmem + d_col, ad, sdesc(g0 + G_LO + step, 128, g_sbo), id, 1u);
+                    mma<TF>(tmem + d_col, sdesc(a0 + A_LO + step, 128, a_sbo), gd, id, 1u);
+                }
+            }
+            mma_commit(&s_bar);
+        }
+        const bool ok = mbar_wait(&s_bar, phase);
+        phase ^= 1;
+        tc_fence_after();
+        if (!ok && tid == 0) atomicExch(a.error_flag, 2);
+        return ok;
+    };
+    // all threads: operand writes visible to the tensor cores, tensor-memory reads done
+    auto handoff = [&]() {
+        async_proxy_fence();
+        tc_fence_before();
+        __syncthreads();
+    };
+
+    for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+        int lo = 0, hi = a.njobs - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (a.jobs[mid].tile_base <= tile) lo = mid; else hi = mid - 1;
+        }
+        const TcJob& job = a.jobs[lo];
+        const int W = job.width, Hh = job.height;
+        const int pw = pad_size(W, B, S), ph = pad_size(Hh, B, S);
+        const int pnx = (pw - B) / S + 1;
+        const int ox = (pw - W) / 2, oy = (ph - Hh) / 2;
+        const int lt = tile - job.tile_base;
+        const int by = lt / job.ntx, tx = lt - by * job.ntx;
+        const int bx0 = tx * TB;
+        const int nb = min(TB, pnx - bx0);  // blocks of this tile
+        const int py0 = by * S, px0 = bx0 * S;
+
+        // ---- stage the input rows of the tile: [t][y][0, PWID)
+        for (int i = tid; i < T * B * PWID; i += NT) {
+            const int t = i / (B * PWID), rem = i - t * B * PWID;
+            const int y = rem / PWID, c = rem - y * PWID;
+            const int px = min(px0 + c, pw - 1);
+            s_patch[i] = load_sample(job.src[t], (long long)mirror(py0 + y - oy, Hh) * job.src_stride +
+                                                     mirror(px - ox, W), P.kind);
+        }
+        __syncthreads();
+        // ---- A1: windowed rows, [t][row = blk * B + y][x]
+        {
+            const int blk = row / B, y = row % B;
+#pragma unroll
+            for (int t = 0; t < T; ++t) {
+#pragma unroll
+                for (int x8 = 0; x8 < B / 16; ++x8) {
+                    const int xb = half * (B / 2) + x8 * 8;
+                    float v[8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+                        v[i] = s_win[(t * B + y) * B + xb + i] * s_patch[(t * B + y) * PWID + blk * S + xb + i];
+                    put8<MODE>(a_hi, A_LO, t * 128 * B + op_index<ESZ>(row, xb, B), v);
+                }
+            }
+        }
+        handoff();
+        bool ok = true;
+        for (int t = 0; t < T && ok; ++t)  // D1[t] = rows of slice t
+            ok = gemm(C_D1 + t * B, t * 128 * B, B, L::g1, B, B / KSTEP);
+        if (__syncthreads_or(!ok)) {
+            s_fail_any = true;
+            break;
+        }
+
+        // ---- A2[(blk, kx)][(t, c, y)] from the packed row spectra
+        {
+            const int blk = row / B, y = row % B;
+#pragma unroll
+            for (int t = 0; t < T; ++t) {
+#pragma unroll
+                for (int j8 = 0; j8 < B / 16; ++j8) {
+                    const int jb = half * (B / 2) + j8 * 8;
+                    float v[8];
+                    tmem_ld8(tmem + lane_base + C_D1 + t * B + jb, v);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        const int j = jb + i;
+                        const int kx = j == 0 ? 0 : (j == 1 ? B / 2 : j >> 1);
+                        const int c = j < 2 ? 0 : (j & 1);
+                        put<MODE>(a_hi, A_LO, op_index<ESZ>(blk * B + kx, (t * 2 + c) * B + y, K2), v[i]);
+                        if (j < 2) put<MODE>(a_hi, A_LO, op_index<ESZ>(blk * B + kx, (t * 2 + 1) * B + y, K2), 0.0f);
+                    }
+                }
+            }
+        }
+        handoff();
+        ok = gemm(C_D2, 0, K2, L::g2, K2, K2 / KSTEP);
+        if (__syncthreads_or(!ok)) {
+            s_fail_any = true;
+            break;
+        }
+
+        // ---- zero-mean, gain, temporal inverse of the centre frame -> A4[(blk, kx)][(c, ky)]
+        {
+            const int blk = row / B, kx = row % B;
+            float z00;
+            tmem_ld1(tmem + lane_base + C_D2, z00);  // Re Z(kt 0, ky 0) of this row
+            tmem_wait_ld();
+            const float dc = __shfl_sync(0xffffffffu, z00, (tid & 31) & ~(B - 1) & 31);
+            const float g = P.g_div != 0.0f ? __fdiv_rn(dc, P.g_div) : 0.0f;
+            // tensor-memory loads are warp-wide: every lane loads, rows kx > B/2 and blocks past the tile end discard
+            const bool active = kx <= B / 2 && blk < nb;
+            const int kxc = kx <= B / 2 ? kx : B / 2;
+#pragma unroll
+            for (int k8 = 0; k8 < B / 16; ++k8) {
+                const int kb = half * (B / 2) + k8 * 8;
+                float yr[8], yi[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) yr[i] = yi[i] = 0.0f;
+#pragma unroll
+                for (int kt = 0; kt < T; ++kt) {
+                    float zr[8], zi[8];
+                    tmem_ld8(tmem + lane_base + C_D2 + (kt * 2) * B + kb, zr);
+                    tmem_ld8(tmem + lane_base + C_D2 + (kt * 2 + 1) * B + kb, zi);
+                    tmem_wait_ld();
+                    // e^{+2 pi i kt r / T}
+                    float sn, cs;
+                    sincospif(2.0f * (float)((kt * R) % T) / (float)T, &sn, &cs);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        const int tb = (kxc * T + kt) * B + kb + i;
+                        const float wr = s_wf[2 * tb], wi = s_wf[2 * tb + 1];
+                        const float dre = fmaf(-g, wr, zr[i]), dim = fmaf(-g, wi, zi[i]);
+                        const float psd = fmaf(dim, dim, dre * dre);
+                        const float s = s_sig[tb];
+                        const float m = FC == kFilterWiener ? gain<0>(psd, s, P) : gain_rt(P.filter_type, psd, s, P);
+                        const float ur = fmaf(m, dre, g * wr), ui = fmaf(m, dim, g * wi);
+                        yr[i] += ur * cs - ui * sn;
+                        yi[i] += ur * sn + ui * cs;
+                    }
+                }
+                if (active) {
+                    put8<MODE>(a_hi, A_LO, op_index<ESZ>(row, kb, 2 * B), yr);
+                    put8<MODE>(a_hi, A_LO, op_index<ESZ>(row, B + kb, 2 * B), yi);
+                }
+            }
+        }
+        handoff();
+        ok = gemm(C_D4, 0, 2 * B, L::g4, 2 * B, 2 * B / KSTEP);
+        if (__syncthreads_or(!ok)) {
+            s_fail_any = true;
+            break;
+        }
+
+        // ---- A5[(blk, y)][j]: inverse column outputs repacked for c2r
+        {
+            const int blk = row / B, kx = row % B;
+            float vr[B / 2], vi[B / 2];
+#pragma unroll
+            for (int y8 = 0; y8 < B / 16; ++y8) {
+                float t0[8], t1[8];
+                tmem_ld8(tmem + lane_base + C_D4 + half * (B / 2) + y8 * 8, t0);
+                tmem_ld8(tmem + lane_base + C_D4 + B + half * (B / 2) + y8 * 8, t1);
+                tmem_wait_ld();
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    vr[y8 * 8 + i] = t0[i];
+                    vi[y8 * 8 + i] = t1[i];
+                }
+            }
+            if (kx <= B / 2) {
+                const int jr = kx == 0 ? 0 : (kx == B / 2 ? 1 : 2 * kx);
+#pragma unroll
+                for (int i = 0; i < B / 2; ++i) {
+                    const int y = half * (B / 2) + i;
+                    put<MODE>(a_hi, A_LO, op_index<ESZ>(blk * B + y, jr, B), vr[i]);
+                    if (kx != 0 && kx != B / 2) put<MODE>(a_hi, A_LO, op_index<ESZ>(blk * B + y, jr + 1, B), vi[i]);
+                }
+            }
+        }
+        handoff();
+        ok = gemm(C_D5, 0, B, L::g5, B, B / KSTEP);
+        if (__syncthreads_or(!ok)) {
+            s_fail_any = true;
+            break;
+        }
+
+        // ---- synthesis window and overlap-add of the tile
+        {
+            const int blk = row / B, y = row % B;
+#pragma unroll
+            for (int x8 = 0; x8 < B / 16; ++x8) {
+                const int xb = half * (B / 2) + x8 * 8;
+                float v[8];
+                tmem_ld8(tmem + lane_base + C_D5 + xb, v);
+                tmem_wait_ld();
+                if (blk < nb) {
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+                        atomicAdd(&s_ola[y * PWID + blk * S + xb + i], v[i] * s_wsyn[y * B + xb + i]);
+                }
+            }
+        }
+        tc_fence_before();
+        __syncthreads();
+        for (int i = tid; i < B * PWID; i += NT) {
+            const int y = i / PWID, c = i - y * PWID;
+            const int py = py0 + y, px = px0 + c;
+            const float v = s_ola[i];
+            s_ola[i] = 0.0f;
+            if (c < (nb - 1) * S + B && py >= oy && py < oy + Hh && px >= ox && px < ox + W)
+                atomicAdd(job.acc + (long long)(py - oy) * W + (px - ox), v);
+        }
+        // the next tile's first barrier orders these reads before the patch and tile reuse
+    }
+    // after a wait that ran out, give the tensor cores one more bounded wait before freeing their memory
+    if (s_fail_any) mbar_wait(&s_bar, phase);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(256) : "memory");
+}
+
+// accumulator planes -> output samples (store_frame, cpu_source/getframe_impl.cpp:177-221)
+__global__ void __launch_bounds__(256) dfttest_tc_finalize(const __grid_constant__ TcArgs a) {
+    const int j = blockIdx.y;
+    const TcJob& job = a.jobs[j];
+    const long long n = (long long)job.width * job.height;
+    const float inv_scale = 1.0f / a.p.scale;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(i / job.width), x = (int)(i - (long long)y * job.width);
+        store_sample(job.dst, (long long)y * job.dst_stride + x, job.acc[i], a.p.kind, a.p.scale, a.p.peak,
+                     a.p.kind == kF32 ? 0.0f : inv_scale);
+    }
+}
+
+}  // namespace dft2

@@ -90,6 +90,9 @@ class Clip(ctypes.Structure):
 
 BATCH_TUNE = 1
 
+# dfttest2_b200_set_precision modes
+PRECISION = {"fp32": 0, "tc_bf16x3": 1, "tc_tf32": 2, "tc_bf16": 3}
+
 # every symbol include/dfttest2_b200.h declares, with its ctypes signature
 SIGNATURES = {
     "dfttest2_b200_params_init": (None, [POINTER(Params)]),
@@ -103,6 +106,7 @@ SIGNATURES = {
     ),
     "dfttest2_b200_process_planes_sigma": (c_int, [c_void_p, POINTER(Plane), c_int, c_int, c_int, c_void_p, c_void_p]),
     "dfttest2_b200_backward_planes": (c_int, [c_void_p, POINTER(GradPlane), c_int, c_void_p, c_void_p, c_void_p]),
+    "dfttest2_b200_set_precision": (c_int, [c_void_p, c_int]),
     "dfttest2_b200_batch_create": (c_int, [POINTER(Clip), c_int, c_int, POINTER(c_void_p)]),
     "dfttest2_b200_batch_run": (c_int, [c_void_p, c_void_p]),
     "dfttest2_b200_batch_describe": (c_int, [c_void_p, ctypes.c_char_p, c_int]),

@@ -66,6 +66,15 @@ class Filter:
         self.radius = 0 if radius is None else int(radius)
         self._lib = lib
 
+    def set_precision(self, mode: str) -> None:
+        """Arithmetic of the block transforms: "fp32" (CUDA-core FFT codelets,
+        the default) or a tensor-core form "tc_bf16x3", "tc_tf32", "tc_bf16"
+        (dfttest2_b200_set_precision)."""
+        if mode not in _lib.PRECISION:
+            raise Error(f"unknown precision mode {mode!r}; one of {sorted(_lib.PRECISION)}")
+        _lib.check(self._lib.dfttest2_b200_set_precision(self.handle, _lib.PRECISION[mode]))
+        self.precision = mode
+
     def close(self):
         if self.handle:
             self._lib.dfttest2_b200_free(self.handle)
