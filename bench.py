@@ -72,6 +72,16 @@ def workload_args():
     return plugin_arguments(**captured)
 
 
+def workload_config(frames_per_gpu, world, bytes_in):
+    """The `config` object both arms print (same workload, same keys)."""
+    frame_bytes = (W * H + 2 * (W // 2) * (H // 2)) * 2
+    return {"workload": "YUV420P16 1920x1080 + 960x540 chroma, 64 frames/GPU, sbsize16 sosize12 tbsize3, "
+                        "ftype0, slocation 12->4, zero-mean, all planes",
+            "frames_per_gpu": frames_per_gpu,
+            "l2": f"inputs {(bytes_in or frame_bytes * frames_per_gpu) / 1e6:.0f} MB/GPU > 126 MB L2, no flush",
+            "parallelism": f"frame shards x{world}"}
+
+
 def blocks_per_frame():
     from dfttest2_b200.clip import YUV420P16, plane_dims
 
@@ -241,7 +251,7 @@ def run_reference(opts, rank, world):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "frames/s", "n_gpus": world,
         "steps": opts.steps, "warmup": opts.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "YUV420P16 1920x1080 (+960x540 chroma), sbsize16 sosize12 tbsize3 ftype0 slocation"},
+        "config": workload_config(FRAMES, world, 0),
         "cpu_baseline": base, "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0,
                                        "d2h_bytes_per_step": 0}}))
 
@@ -514,10 +524,7 @@ def main():
         "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": opts.steps,
         "warmup": opts.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded sinusoids + gaussian + 1% salt-pepper)",
-        "config": {"workload": "YUV420P16 1920x1080 + 960x540 chroma, 64 frames/GPU, sbsize16 sosize12 tbsize3, "
-                               "ftype0, slocation 12->4, zero-mean, all planes",
-                   "frames_per_gpu": hi - lo, "l2": f"inputs {bytes_in / 1e6:.0f} MB/GPU > 126 MB L2, no flush",
-                   "parallelism": f"frame shards x{world}"},
+        "config": workload_config(hi - lo, world, bytes_in),
         "e2e": {"value": e2e_frames / e2e_s, "unit": "frames/s", "h2d_bytes_per_step": bytes_in,
                 "d2h_bytes_per_step": bytes_in, "path": "dfttest2_b200_process_clip_host, pinned host memory"},
         "gpu_launches": 2 * opts.steps,

@@ -401,8 +401,12 @@ void build_gmat(std::vector<char>& img) {
     auto put = [&](int off, int n, int k, int KT, double v) {
         const int idx = off + dft2::op_index<ESZ>(n, k, KT);
         if (MODE == dft2::kTcTf32) {
+            // round to the 10-bit tf32 mantissa, nearest even (the tensor cores would truncate)
             const float f = (float)v;
-            std::memcpy(&img[(size_t)idx * 4], &f, 4);
+            uint32_t u;
+            std::memcpy(&u, &f, 4);
+            u = (u + 0x0FFFu + ((u >> 13) & 1u)) & ~0x1FFFu;
+            std::memcpy(&img[(size_t)idx * 4], &u, 4);
         } else {
             const __nv_bfloat16 h = __float2bfloat16_rn((float)v);
             std::memcpy(&img[(size_t)idx * 2], &h, 2);
@@ -538,10 +542,13 @@ int launch_tc(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, f
     if (smem > 227 * 1024) return fail(DFTTEST2_B200_EINVAL, "block step too large for the tensor-core form");
     TcKernelFn kern = f->filter_type == 0 ? v.wiener : v.generic;
     CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     int per_sm = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
     if (per_sm < 1) return fail(DFTTEST2_B200_ECUDA, "tensor-core kernel does not fit on an SM");
-    const int grid = std::max(1, std::min(a.ntiles, f->num_sms * std::min(per_sm, 2)));
+    // two CTAs per SM (register bound of the kernel; tensor memory holds 2 x 256 columns); the occupancy
+    // query can report one for this shared-memory size while two are resident, so it is not used for the grid
+    const int grid = std::max(1, std::min(a.ntiles, f->num_sms * 2));
     kern<<<grid, 256, smem, stream>>>(a);
     CUDA_TRY(cudaGetLastError());
     dim3 fg((unsigned)std::max<long long>(1, std::min<long long>(64, (acc / jobs.size() + 255) / 256)),

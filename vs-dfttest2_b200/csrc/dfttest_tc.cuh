@@ -154,11 +154,18 @@ struct Operand {
     static constexpr bool SPLIT = MODE == kTcBf16x3;
 };
 
+// fp32 -> tf32, rounded to nearest (the tensor cores would truncate the low mantissa bits)
+__device__ __forceinline__ float to_tf32(float v) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
+    return __uint_as_float(r);
+}
+
 // operand buffers hold a hi plane and (BF16X3) a lo plane `lo_off` bytes later
 template <int MODE>
 __device__ __forceinline__ void put(char* base, int lo_off, int idx, float v) {
     if constexpr (MODE == kTcTf32) {
-        reinterpret_cast<float*>(base)[idx] = v;
+        reinterpret_cast<float*>(base)[idx] = to_tf32(v);
     } else {
         const __nv_bfloat16 h = __float2bfloat16_rn(v);
         reinterpret_cast<__nv_bfloat16*>(base)[idx] = h;
@@ -173,8 +180,9 @@ __device__ __forceinline__ void put8(char* base, int lo_off, int idx, const floa
     if constexpr (MODE == kTcTf32) {
         float4* p = reinterpret_cast<float4*>(reinterpret_cast<float*>(base) + idx);
         // idx is a multiple of 4; the two halves lie in consecutive core matrices along K
-        p[0] = make_float4(v[0], v[1], v[2], v[3]);
-        reinterpret_cast<float4*>(reinterpret_cast<float*>(base) + idx + 32)[0] = make_float4(v[4], v[5], v[6], v[7]);
+        p[0] = make_float4(to_tf32(v[0]), to_tf32(v[1]), to_tf32(v[2]), to_tf32(v[3]));
+        reinterpret_cast<float4*>(reinterpret_cast<float*>(base) + idx + 32)[0] =
+            make_float4(to_tf32(v[4]), to_tf32(v[5]), to_tf32(v[6]), to_tf32(v[7]));
     } else {
         __align__(16) __nv_bfloat16 h[8], l[8];
 #pragma unroll
@@ -284,29 +292,38 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc_kernel(const __grid_constan
     uint32_t phase = 0;
     bool s_fail_any = false;
 
-    // issue `nk` K steps of D(128 x N) = A(128 x K) * G(N x K)^T, commit, wait
-    auto gemm = [&](uint32_t d_col, int a_off, int a_kt, int g_off, int n, int nk) -> bool {
+    // issue `nk` K steps of D(128 x N) = A(128 x K) * G(N x K)^T for `count` operand slices
+    // (slice i: A at a_off + i * a_step elements, D at d_col + i * d_step columns), one commit;
+    // thread 0 waits for the tensor cores, the others at the barrier.  Returns false on a timeout.
+    auto gemm = [&](uint32_t d_col, int a_off, int a_kt, int g_off, int n, int nk, int count = 1, int a_step = 0,
+                    int d_step = 0) -> bool {
+        bool ok = true;
         if (tid == 0) {
             tc_fence_after();
             const uint32_t id = idesc(TF ? 2 : 1, 128, n);
-            const uint32_t a0 = smem_addr(a_hi) + a_off * ESZ, g0 = smem_addr(g_hi) + g_off * ESZ;
-            const uint32_t a_sbo = (a_kt * ESZ / 16) * 128, g_sbo = (a_kt * ESZ / 16) * 128;
-            for (int s = 0; s < nk; ++s) {
-                const uint32_t step = s * 256;  // two core matrices along K per MMA
-                const uint64_t ad = sdesc(a0 + step, 128, a_sbo), gd = sdesc(g0 + step, 128, g_sbo);
-                mma<TF>(tmem + d_col, ad, gd, id, s > 0 ? 1u : 0u);
-                if constexpr (MODE == kTcBf16x3) {
-                    mma<TF>(tmem + d_col, ad, sdesc(g0 + G_LO + step, 128, g_sbo), id, 1u);
-                    mma<TF>(tmem + d_col, sdesc(a0 + A_LO + step, 128, a_sbo), gd, id, 1u);
+            const uint32_t g0 = smem_addr(g_hi) + g_off * ESZ;
+            const uint32_t sbo = (a_kt * ESZ / 16) * 128;
+            for (int sl = 0; sl < count; ++sl) {
+                const uint32_t a0 = smem_addr(a_hi) + (a_off + sl * a_step) * ESZ;
+                const uint32_t d = tmem + d_col + sl * d_step;
+                for (int s = 0; s < nk; ++s) {
+                    const uint32_t step = s * 256;  // two core matrices along K per MMA
+                    const uint64_t ad = sdesc(a0 + step, 128, sbo), gd = sdesc(g0 + step, 128, sbo);
+                    mma<TF>(d, ad, gd, id, s > 0 ? 1u : 0u);
+                    if constexpr (MODE == kTcBf16x3) {
+                        mma<TF>(d, ad, sdesc(g0 + G_LO + step, 128, sbo), id, 1u);
+                        mma<TF>(d, sdesc(a0 + A_LO + step, 128, sbo), gd, id, 1u);
+                    }
                 }
             }
             mma_commit(&s_bar);
+            ok = mbar_wait(&s_bar, phase);
+            if (!ok) atomicExch(a.error_flag, 2);
         }
-        const bool ok = mbar_wait(&s_bar, phase);
         phase ^= 1;
+        const bool fail = __syncthreads_or(!ok);
         tc_fence_after();
-        if (!ok && tid == 0) atomicExch(a.error_flag, 2);
-        return ok;
+        return !fail;
     };
     // all threads: operand writes visible to the tensor cores, tensor-memory reads done
     auto handoff = [&]() {
@@ -332,13 +349,14 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc_kernel(const __grid_constan
         const int nb = min(TB, pnx - bx0);  // blocks of this tile
         const int py0 = by * S, px0 = bx0 * S;
 
-        // ---- stage the input rows of the tile: [t][y][0, PWID)
-        for (int i = tid; i < T * B * PWID; i += NT) {
-            const int t = i / (B * PWID), rem = i - t * B * PWID;
-            const int y = rem / PWID, c = rem - y * PWID;
-            const int px = min(px0 + c, pw - 1);
-            s_patch[i] = load_sample(job.src[t], (long long)mirror(py0 + y - oy, Hh) * job.src_stride +
-                                                     mirror(px - ox, W), P.kind);
+        // ---- stage the input rows of the tile: [t][y][0, PWID), one warp per row
+        for (int r = warp; r < T * B; r += NT / 32) {
+            const int t = r / B, y = r - t * B;
+            const long long rowoff = (long long)mirror(py0 + y - oy, Hh) * job.src_stride;
+            for (int c = tid & 31; c < PWID; c += 32) {
+                const int px = min(px0 + c, pw - 1);
+                s_patch[r * PWID + c] = load_sample(job.src[t], rowoff + mirror(px - ox, W), P.kind);
+            }
         }
         __syncthreads();
         // ---- A1: windowed rows, [t][row = blk * B + y][x]
@@ -358,10 +376,8 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc_kernel(const __grid_constan
             }
         }
         handoff();
-        bool ok = true;
-        for (int t = 0; t < T && ok; ++t)  // D1[t] = rows of slice t
-            ok = gemm(C_D1 + t * B, t * 128 * B, B, L::g1, B, B / KSTEP);
-        if (__syncthreads_or(!ok)) {
+        bool ok = gemm(C_D1, 0, B, L::g1, B, B / KSTEP, T, 128 * B, B);  // D1[t] = rows of slice t
+        if (!ok) {
             s_fail_any = true;
             break;
         }
@@ -390,7 +406,7 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc_kernel(const __grid_constan
         }
         handoff();
         ok = gemm(C_D2, 0, K2, L::g2, K2, K2 / KSTEP);
-        if (__syncthreads_or(!ok)) {
+        if (!ok) {
             s_fail_any = true;
             break;
         }
@@ -442,7 +458,7 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc_kernel(const __grid_constan
         }
         handoff();
         ok = gemm(C_D4, 0, 2 * B, L::g4, 2 * B, 2 * B / KSTEP);
-        if (__syncthreads_or(!ok)) {
+        if (!ok) {
             s_fail_any = true;
             break;
         }
@@ -475,7 +491,7 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc_kernel(const __grid_constan
         }
         handoff();
         ok = gemm(C_D5, 0, B, L::g5, B, B / KSTEP);
-        if (__syncthreads_or(!ok)) {
+        if (!ok) {
             s_fail_any = true;
             break;
         }
@@ -498,13 +514,16 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc_kernel(const __grid_constan
         }
         tc_fence_before();
         __syncthreads();
-        for (int i = tid; i < B * PWID; i += NT) {
-            const int y = i / PWID, c = i - y * PWID;
-            const int py = py0 + y, px = px0 + c;
-            const float v = s_ola[i];
-            s_ola[i] = 0.0f;
-            if (c < (nb - 1) * S + B && py >= oy && py < oy + Hh && px >= ox && px < ox + W)
-                atomicAdd(job.acc + (long long)(py - oy) * W + (px - ox), v);
+        for (int y = warp; y < B; y += NT / 32) {
+            const int py = py0 + y;
+            const bool rin = py >= oy && py < oy + Hh;
+            float* accrow = job.acc + (long long)(py - oy) * W - ox;
+            for (int c = tid & 31; c < PWID; c += 32) {
+                const int px = px0 + c;
+                const float v = s_ola[y * PWID + c];
+                s_ola[y * PWID + c] = 0.0f;
+                if (rin && c < (nb - 1) * S + B && px >= ox && px < ox + W) atomicAdd(accrow + px, v);
+            }
         }
         // the next tile's first barrier orders these reads before the patch and tile reuse
     }
