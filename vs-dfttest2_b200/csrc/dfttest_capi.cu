@@ -84,6 +84,7 @@ Variant select_variant(int B, int T) {
     // DFTTEST2_B200_WARPS=16 selects the one-CTA-per-SM shape for 16x16x3
     const char* env = std::getenv("DFTTEST2_B200_WARPS");
     if (env && B == 16 && T == 3 && std::atoi(env) == 16) return make_variant<16, 3, 16>();
+    if (env && B == 16 && T == 3 && std::atoi(env) == 4) return make_variant<16, 3, 4, 4>();
     switch (B) {
 #ifndef DFTTEST2_B200_ONLY_B16
     case 8:
@@ -131,7 +132,10 @@ std::vector<Variant> candidate_variants(int B, int T) {
     if (B == 32 && T == 3) v.push_back(make_variant<32, 3, 4, 2>());
 #endif
     if (B == 16 && T == 1) v.push_back(make_variant<16, 1, 8, 2>());
-    if (B == 16 && T == 3) v.push_back(make_variant<16, 3, 16>());
+    if (B == 16 && T == 3) {
+        v.push_back(make_variant<16, 3, 16>());
+        v.push_back(make_variant<16, 3, 4, 4>());
+    }
     return v;
 }
 
