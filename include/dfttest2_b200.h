@@ -122,6 +122,27 @@ int dfttest2_b200_process_clip_host(dfttest2_b200_filter* f, const void* src, pt
                                     ptrdiff_t dst_frame_bytes, int nframes, int width, int height, int sample_type,
                                     int bits_per_sample);
 
+/* One plane of a clip in host memory: frame i at src + i*src_frame_bytes,
+ * rows src_stride bytes apart (likewise dst). */
+typedef struct dfttest2_b200_host_plane {
+    const void* src;
+    ptrdiff_t src_stride;
+    ptrdiff_t src_frame_bytes;
+    void* dst;
+    ptrdiff_t dst_stride;
+    ptrdiff_t dst_frame_bytes;
+    int width;
+    int height;
+} dfttest2_b200_host_plane;
+
+/* Whole-clip host path over several planes of one sample format (the planes
+ * of a YUV clip): one upload / filter / download pipeline for all of them, so
+ * it fills and drains once; each chunk of frames filters every plane's
+ * frames in one launch.  Same semantics per plane as
+ * dfttest2_b200_process_clip_host, which is this call with one plane. */
+int dfttest2_b200_process_clip_planes_host(dfttest2_b200_filter* f, const dfttest2_b200_host_plane* planes,
+                                           int nplanes, int nframes, int sample_type, int bits_per_sample);
+
 /* Differentiable path (float planes).  The reference has no gradient; these
  * serve training the sigma array and backpropagating through the filter.
  *

@@ -90,7 +90,8 @@ def test_struct_layouts_match_the_header(tmp_path):
     import subprocess
 
     structs = {"dfttest2_b200_params": _lib.Params, "dfttest2_b200_plane": _lib.Plane,
-               "dfttest2_b200_grad_plane": _lib.GradPlane, "dfttest2_b200_clip": _lib.Clip}
+               "dfttest2_b200_grad_plane": _lib.GradPlane, "dfttest2_b200_clip": _lib.Clip,
+               "dfttest2_b200_host_plane": _lib.HostPlane}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "dfttest2_b200.h"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

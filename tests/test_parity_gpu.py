@@ -199,3 +199,30 @@ def test_batch_of_planes_matches_single_launches(cuda_device):
     assert d.max() <= 1
     f64 = O.fp64_plane(O.clip_frames(clip, 5, 1), args, 16)
     check(batch[5], O.quantize(f64, np.uint16, 16), 16, "batch frame 5")
+
+
+@pytest.mark.parametrize("nframes", [1, 3, 13, 40])
+def test_multi_plane_host_pipeline_equals_device_path(nframes, cuda_device):
+    """dfttest2_b200_process_clip_planes_host (one pipeline over the three
+    planes of a YUV420P16 clip, chunks ramping 4, 8, 16, ..., 8, 4) gives the
+    device path's result for every frame, including the clip-end clamp
+    (within 1 LSB: the launches split planes into units differently, which
+    reorders the overlap-add sums at unit edges)."""
+    import torch
+
+    from dfttest2_b200.plugin import Filter
+
+    args = plugin_arguments(ftype=0, sigma=8.0, sbsize=16, sosize=12, tbsize=3)
+    rng = np.random.default_rng(nframes)
+    planes = [np.round(np.clip(0.5 + 0.2 * rng.standard_normal((nframes, h, w)), 0, 1) * 65535).astype(np.uint16)
+              for (w, h) in ((160, 96), (80, 48), (80, 48))]
+    flt = Filter(device_id=0, **args)
+    try:
+        host = flt.process_clip_planes_host(planes, 0, 16)
+        for p, h in zip(planes, host):
+            dev = flt.process_clip_device(torch.from_numpy(p.view(np.int16)).cuda(0), 0, 16)
+            torch.cuda.synchronize()
+            d = np.abs(dev.cpu().numpy().view(np.uint16).astype(np.int64) - h.astype(np.int64))
+            assert d.max() <= 1 and (d == 0).mean() > 0.99
+    finally:
+        flt.close()

@@ -427,18 +427,15 @@ void build_gmat(std::vector<char>& img) {
             const double ang = 2.0 * pi * k * x / B;
             put(L::g1, j, x, B, j < 2 ? std::cos(ang) : ((j & 1) ? -std::sin(ang) : std::cos(ang)));
         }
-    // G2: F_t (x) F_y in real form, [(kt, c', ky)][(t, c, y)]
-    constexpr int K2 = L::K2;
-    for (int kt = 0; kt < T; ++kt)
-        for (int cp = 0; cp < 2; ++cp)
-            for (int ky = 0; ky < B; ++ky)
-                for (int t = 0; t < T; ++t)
-                    for (int c = 0; c < 2; ++c)
-                        for (int y = 0; y < B; ++y) {
-                            const double th = 2.0 * pi * ((double)(kt * t % T) / T + (double)(ky * y % B) / B);
-                            const double v = cp == c ? std::cos(th) : (c == 1 ? std::sin(th) : -std::sin(th));
-                            put(L::g2, (kt * 2 + cp) * B + ky, (t * 2 + c) * B + y, K2, v);
-                        }
+    // G2: forward complex DFT over y in real form, [(c', ky)][(c, y)]
+    for (int cp = 0; cp < 2; ++cp)
+        for (int ky = 0; ky < B; ++ky)
+            for (int c = 0; c < 2; ++c)
+                for (int y = 0; y < B; ++y) {
+                    const double th = 2.0 * pi * (double)(ky * y % B) / B;
+                    const double v = cp == c ? std::cos(th) : (c == 1 ? std::sin(th) : -std::sin(th));
+                    put(L::g2, cp * B + ky, c * B + y, 2 * B, v);
+                }
     // G4: inverse complex DFT over y, [(c', y)][(c, ky)]
     for (int cp = 0; cp < 2; ++cp)
         for (int y = 0; y < B; ++y)
@@ -999,56 +996,93 @@ int dfttest2_b200_process_plane_host(dfttest2_b200_filter* f, const dfttest2_b20
     return 0;
 }
 
-int dfttest2_b200_process_clip_host(dfttest2_b200_filter* f, const void* src, ptrdiff_t src_stride,
-                                    ptrdiff_t src_frame_bytes, void* dst, ptrdiff_t dst_stride,
-                                    ptrdiff_t dst_frame_bytes, int nframes, int width, int height, int sample_type,
-                                    int bits_per_sample) {
-    if (!f || !src || !dst || nframes <= 0) return fail(DFTTEST2_B200_EINVAL, "invalid argument");
+int dfttest2_b200_process_clip_planes_host(dfttest2_b200_filter* f, const dfttest2_b200_host_plane* hp, int nplanes,
+                                           int nframes, int sample_type, int bits_per_sample) {
+    if (!f || !hp || nplanes <= 0 || nframes <= 0) return fail(DFTTEST2_B200_EINVAL, "invalid argument");
     if (int rc = check_format(sample_type, bits_per_sample)) return rc;
-    DeviceGuard dg(f->device);
     const int bps = bytes_of(sample_type, bits_per_sample);
-    const size_t row = (size_t)width * bps;
-    const size_t frame = row * height;
+    std::vector<size_t> row(nplanes), frame(nplanes), src_off(nplanes), out_off(nplanes);
+    size_t src_total = 0, out_chunk = 0;
+    for (int i = 0; i < nplanes; ++i) {
+        if (!hp[i].src || !hp[i].dst || hp[i].width <= 0 || hp[i].height <= 0)
+            return fail(DFTTEST2_B200_EINVAL, "invalid argument");
+        row[i] = (size_t)hp[i].width * bps;
+        frame[i] = row[i] * hp[i].height;
+        src_off[i] = src_total;
+        src_total += frame[i] * nframes;
+        out_off[i] = out_chunk;
+        out_chunk += frame[i];  // per output frame of the chunk
+    }
+    DeviceGuard dg(f->device);
     const int r = f->radius;
     SlotGuard sg(f);
     Slot& s = sg.slot();
-    // Three-stream pipeline over chunks of output frames: uploads (stream
-    // `up`), filtering (slot stream) and downloads (stream `down`) of
-    // consecutive chunks overlap.  Every source frame is uploaded once into a
+    // Chunks of output frames ramp up (4, 8, 16, ...) and down at the end so
+    // that the first upload and the last download, which nothing overlaps,
+    // stay short.  Uploads (stream `up`), filtering of every plane's frames of
+    // a chunk in one launch (slot stream) and downloads (stream `down`) of
+    // consecutive chunks overlap; every source frame is uploaded once into a
     // dense device array; outputs alternate between two chunk buffers.
-    const int chunk = std::max(1, std::min(nframes, 16));
-    if (int rc = ensure_bytes(s.d_frames, s.frames_cap, frame * ((size_t)nframes + 2 * chunk), s.done)) return rc;
+    constexpr int kMaxChunk = 16;
+    std::vector<int> chunks;
+    {
+        int left = nframes;
+        for (int c : {4, 8}) {
+            if (left <= 0) break;
+            const int take = std::min(c, left);
+            chunks.push_back(take);
+            left -= take;
+        }
+        std::vector<int> tail;
+        for (int c : {4, 8}) {  // the last chunks, smallest last
+            if (left <= 0) break;
+            const int take = std::min(c, left);
+            tail.push_back(take);
+            left -= take;
+        }
+        while (left > 0) {
+            const int take = std::min(kMaxChunk, left);
+            chunks.push_back(take);
+            left -= take;
+        }
+        chunks.insert(chunks.end(), tail.rbegin(), tail.rend());
+    }
+    if (int rc = ensure_bytes(s.d_frames, s.frames_cap, src_total + 2 * kMaxChunk * out_chunk, s.done)) return rc;
     CUDA_TRY(cudaEventSynchronize(s.done));
-    uint8_t* dframes = (uint8_t*)s.d_frames;
-    uint8_t* dout[2] = {dframes + frame * nframes, dframes + frame * ((size_t)nframes + chunk)};
-    const uint8_t* hsrc = (const uint8_t*)src;
-    uint8_t* hdst = (uint8_t*)dst;
+    uint8_t* dsrc = (uint8_t*)s.d_frames;
+    uint8_t* dout[2] = {dsrc + src_total, dsrc + src_total + kMaxChunk * out_chunk};
     float scale, peak;
     int kind;
     scale_peak(sample_type, bits_per_sample, scale, peak, kind);
-    int uploaded = 0;
-    int k = 0;
-    for (int c0 = 0; c0 < nframes; c0 += chunk, ++k) {
-        const int c1 = std::min(nframes, c0 + chunk);
+    int uploaded = 0, c0 = 0;
+    for (size_t k = 0; k < chunks.size(); ++k) {
+        const int c1 = c0 + chunks[k];
         const int need = std::min(nframes, c1 + r);
         for (; uploaded < need; ++uploaded) {
-            CUDA_TRY(cudaMemcpy2DAsync(dframes + frame * uploaded, row, hsrc + src_frame_bytes * uploaded, src_stride,
-                                       row, height, cudaMemcpyHostToDevice, s.up));
+            for (int i = 0; i < nplanes; ++i)
+                CUDA_TRY(cudaMemcpy2DAsync(dsrc + src_off[i] + frame[i] * uploaded, row[i],
+                                           (const uint8_t*)hp[i].src + hp[i].src_frame_bytes * uploaded,
+                                           hp[i].src_stride, row[i], hp[i].height, cudaMemcpyHostToDevice, s.up));
         }
         CUDA_TRY(cudaEventRecord(s.ev_up[k & 1], s.up));
-        std::vector<dfttest2_b200_plane> planes(c1 - c0);
-        for (int n = c0; n < c1; ++n) {
-            dfttest2_b200_plane& p = planes[n - c0];
-            std::memset(&p, 0, sizeof(p));
-            for (int t = 0; t < f->T; ++t) {
-                const int fi = std::min(std::max(n - r + t, 0), nframes - 1);
-                p.src[t] = dframes + frame * fi;
+        uint8_t* ob = dout[k & 1];
+        std::vector<dfttest2_b200_plane> planes;
+        planes.reserve((size_t)(c1 - c0) * nplanes);
+        for (int i = 0; i < nplanes; ++i) {
+            for (int n = c0; n < c1; ++n) {
+                dfttest2_b200_plane p;
+                std::memset(&p, 0, sizeof(p));
+                for (int t = 0; t < f->T; ++t) {
+                    const int fi = std::min(std::max(n - r + t, 0), nframes - 1);
+                    p.src[t] = dsrc + src_off[i] + frame[i] * fi;
+                }
+                p.src_stride = row[i];
+                p.dst = ob + kMaxChunk * out_off[i] + frame[i] * (n - c0);
+                p.dst_stride = row[i];
+                p.width = hp[i].width;
+                p.height = hp[i].height;
+                planes.push_back(p);
             }
-            p.src_stride = row;
-            p.dst = dout[k & 1] + frame * (n - c0);
-            p.dst_stride = row;
-            p.width = width;
-            p.height = height;
         }
         Plan plan;
         if (int rc = make_plan(f, planes.data(), (int)planes.size(), bps, plan)) return rc;
@@ -1057,16 +1091,35 @@ int dfttest2_b200_process_clip_host(dfttest2_b200_filter* f, const void* src, pt
         if (int rc = launch(f, s, plan, kind, scale, peak, s.stream)) return rc;
         CUDA_TRY(cudaEventRecord(s.ev_comp[k & 1], s.stream));
         CUDA_TRY(cudaStreamWaitEvent(s.down, s.ev_comp[k & 1], 0));
-        for (int n = c0; n < c1; ++n) {
-            CUDA_TRY(cudaMemcpy2DAsync(hdst + dst_frame_bytes * n, dst_stride, dout[k & 1] + frame * (n - c0), row, row,
-                                       height, cudaMemcpyDeviceToHost, s.down));
-        }
+        for (int i = 0; i < nplanes; ++i)
+            for (int n = c0; n < c1; ++n)
+                CUDA_TRY(cudaMemcpy2DAsync((uint8_t*)hp[i].dst + hp[i].dst_frame_bytes * n, hp[i].dst_stride,
+                                           ob + kMaxChunk * out_off[i] + frame[i] * (n - c0), row[i], row[i],
+                                           hp[i].height, cudaMemcpyDeviceToHost, s.down));
         CUDA_TRY(cudaEventRecord(s.ev_down[k & 1], s.down));
+        c0 = c1;
     }
     CUDA_TRY(cudaStreamSynchronize(s.down));
     CUDA_TRY(cudaStreamSynchronize(s.stream));
     CUDA_TRY(cudaEventRecord(s.done, s.stream));
     return 0;
+}
+
+int dfttest2_b200_process_clip_host(dfttest2_b200_filter* f, const void* src, ptrdiff_t src_stride,
+                                    ptrdiff_t src_frame_bytes, void* dst, ptrdiff_t dst_stride,
+                                    ptrdiff_t dst_frame_bytes, int nframes, int width, int height, int sample_type,
+                                    int bits_per_sample) {
+    if (!f || !src || !dst || nframes <= 0) return fail(DFTTEST2_B200_EINVAL, "invalid argument");
+    dfttest2_b200_host_plane p;
+    p.src = src;
+    p.src_stride = src_stride;
+    p.src_frame_bytes = src_frame_bytes;
+    p.dst = dst;
+    p.dst_stride = dst_stride;
+    p.dst_frame_bytes = dst_frame_bytes;
+    p.width = width;
+    p.height = height;
+    return dfttest2_b200_process_clip_planes_host(f, &p, 1, nframes, sample_type, bits_per_sample);
 }
 
 int dfttest2_b200_process_planes_sigma(dfttest2_b200_filter* f, const dfttest2_b200_plane* planes, int nplanes,

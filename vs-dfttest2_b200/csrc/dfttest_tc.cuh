@@ -6,12 +6,14 @@
 // frame, synthesis window, overlap-add) on the CUDA cores.
 //
 // A tile is TB = 128 / B neighbouring blocks of one block row.  Per tile:
-//   G1  row r2c         rows (t, blk, y)  K = B (x)           N = B  (packed bins j)
-//   G2  col + temporal  rows (blk, kx)    K = (t, c, y) 2TB   N = (kt, c, ky) 2TB
-//       DFT (F_t (x) F_y in real form; kx padded to B rows, rows kx > B/2 unused)
-//   --  zero-mean, gain, inverse over t of the centre frame (CUDA cores)
-//   G4  inverse col DFT rows (blk, kx)    K = (c, ky) 2B      N = (c, y) 2B
-//   G5  c2r             rows (blk, y)     K = B (packed j)    N = B (x)
+//   G1  row r2c          rows (blk, y)   K = B (x)        N = B (packed bins j)   one product per frame t
+//   G2  column DFT       rows (blk, kx)  K = (c, y) 2B    N = (c, ky) 2B          one product per frame t
+//       (kx padded to B rows, rows kx > B/2 unused; the operand is MN-major so
+//       that each thread writes whole 16-byte chunks of the row spectra it holds)
+//   --  temporal DFT, zero-mean, gain, inverse over t of the centre frame
+//       (CUDA cores; the T products of a bin sit in one tensor-memory lane)
+//   G4  inverse col DFT  rows (blk, kx)  K = (c, ky) 2B   N = (c, y) 2B
+//   G5  c2r              rows (blk, y)   K = B (packed j) N = B (x)   (A MN-major)
 // Packed bins j of a real row: j = 0 -> Re X0, 1 -> Re X_{B/2}, 2k -> Re Xk,
 // 2k + 1 -> Im Xk (k = 1 .. B/2 - 1); c2r ignores Im X0 and Im X_{B/2}.
 //
@@ -27,6 +29,7 @@
 #include <cuda_bf16.h>
 
 #include "dfttest_kernel.cuh"
+#include "dfttest_adjoint.cuh"  // cdft_n
 
 namespace dft2 {
 
@@ -72,10 +75,11 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t 
 }
 
 // instruction descriptor of kind::f16 / kind::tf32: D f32, A and B K-major
-__host__ __device__ constexpr uint32_t idesc(int ab_format, int M, int N) {
+__host__ __device__ constexpr uint32_t idesc(int ab_format, int M, int N, bool a_mn_major = false) {
     return (1u << 4)                       // D format f32
            | ((uint32_t)ab_format << 7)    // A format (1 = bf16, 2 = tf32)
            | ((uint32_t)ab_format << 10)   // B format
+           | ((a_mn_major ? 1u : 0u) << 15)  // A major: 0 = K, 1 = MN
            | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
@@ -146,6 +150,14 @@ __host__ __device__ constexpr int op_index(int m, int k, int KT) {
     return (((m >> 3) * (KT / PER) + k / PER) * 8 + (m & 7)) * PER + (k % PER);
 }
 
+// element (m, k) of an MN-major operand with MT rows: 8 k-rows of 16 bytes (16/ESZ
+// consecutive m) per core matrix; m-groups 128 bytes apart, k-groups MT/(16/ESZ) * 128 bytes
+template <int ESZ>
+__host__ __device__ constexpr int op_index_mn(int m, int k, int MT) {
+    constexpr int PER = 16 / ESZ;
+    return ((k / 8) * (MT / PER) + m / PER) * (8 * PER) + (k % 8) * PER + (m % PER);
+}
+
 // operand store of one value: bf16 hi (+ lo) or tf32 (fp32 bits)
 template <int MODE>
 struct Operand {
@@ -197,6 +209,14 @@ __device__ __forceinline__ void put8(char* base, int lo_off, int idx, const floa
     }
 }
 
+// 8 consecutive M values (m0 a multiple of 8) of one K column of a 128-row MN-major
+// operand (16-bit types: the tensor cores read MN-major operands of bf16, not tf32)
+template <int MODE>
+__device__ __forceinline__ void put8_mn(char* base, int lo_off, int m0, int k, const float (&v)[8]) {
+    static_assert(MODE != kTcTf32, "tf32 operands are K-major");
+    put8<MODE>(base, lo_off, op_index_mn<2>(m0, k, 128), v);
+}
+
 // shared-memory plan of the tensor-core kernel (bytes)
 template <int B, int T, int MODE>
 struct TcLayout {
@@ -204,14 +224,13 @@ struct TcLayout {
     static constexpr int NPLANE = Operand<MODE>::SPLIT ? 2 : 1;
     static constexpr int X = B / 2 + 1;
     static constexpr int TB = 128 / B;       // blocks per tile
-    static constexpr int K2 = 2 * T * B;     // column + temporal stage width
-    // constant operands (N x K each), hi planes then lo planes
-    static constexpr int G1 = B * B, G2 = K2 * K2, G4 = 4 * B * B, G5 = B * B;
+    // constant operands (N x K each, K-major), hi planes then lo planes
+    static constexpr int G1 = B * B, G2 = 4 * B * B, G4 = 4 * B * B, G5 = B * B;
     static constexpr int GELEM = G1 + G2 + G4 + G5;
     static constexpr int g1 = 0, g2 = G1, g4 = G1 + G2, g5 = G1 + G2 + G4;  // element offsets in a plane
     static constexpr int GBYTES = GELEM * ESZ * NPLANE;
-    // A operand region: the largest stage (A1 has T planes of 128 x B)
-    static constexpr int A1 = T * 128 * B, A2 = 128 * K2, A4 = 128 * 2 * B, A5 = 128 * B;
+    // A operand region: the largest stage (A1, A2 have T planes)
+    static constexpr int A1 = T * 128 * B, A2 = T * 128 * 2 * B, A4 = 128 * 2 * B, A5 = 128 * B;
     static constexpr int AELEM = A1 > A2 ? (A1 > A4 ? A1 : A4) : (A2 > A4 ? A2 : A4);
     static constexpr int ABYTES = AELEM * ESZ * NPLANE;
     static constexpr int o_g = 0;
@@ -229,8 +248,7 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc_kernel(const __grid_constan
     using L = TcLayout<B, T, MODE>;
     constexpr bool TF = MODE == kTcTf32;
     constexpr int ESZ = L::ESZ;
-    constexpr int X = L::X, TB = L::TB, K2 = L::K2;
-    constexpr int R = (T - 1) / 2;
+    constexpr int X = L::X, TB = L::TB;
     constexpr int NT = 256;
     constexpr int KSTEP = TF ? 8 : 16;  // K per MMA
     extern __shared__ __align__(128) char tc_smem[];
@@ -295,24 +313,28 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc_kernel(const __grid_constan
     // issue `nk` K steps of D(128 x N) = A(128 x K) * G(N x K)^T for `count` operand slices
     // (slice i: A at a_off + i * a_step elements, D at d_col + i * d_step columns), one commit;
     // thread 0 waits for the tensor cores, the others at the barrier.  Returns false on a timeout.
-    auto gemm = [&](uint32_t d_col, int a_off, int a_kt, int g_off, int n, int nk, int count = 1, int a_step = 0,
-                    int d_step = 0) -> bool {
+    // A is K-major, or MN-major (a_mn) with 128 rows; G is K-major.
+    auto gemm = [&](uint32_t d_col, int a_off, int a_kt, bool a_mn, int g_off, int n, int nk, int count = 1,
+                    int a_step = 0, int d_step = 0) -> bool {
         bool ok = true;
         if (tid == 0) {
             tc_fence_after();
-            const uint32_t id = idesc(TF ? 2 : 1, 128, n);
+            const uint32_t id = idesc(TF ? 2 : 1, 128, n, a_mn);
             const uint32_t g0 = smem_addr(g_hi) + g_off * ESZ;
-            const uint32_t sbo = (a_kt * ESZ / 16) * 128;
+            const uint32_t g_sbo = (a_kt * ESZ / 16) * 128;               // K-major: 8-row group stride
+            const uint32_t a_lbo = a_mn ? (128 * ESZ / 16) * 128 : 128;   // K-direction core-matrix stride
+            const uint32_t a_sbo = a_mn ? 128 : g_sbo;                    // M-direction core-matrix stride
+            const uint32_t a_kstep = a_mn ? (KSTEP / 8) * a_lbo : 256;     // bytes per MMA K step
             for (int sl = 0; sl < count; ++sl) {
                 const uint32_t a0 = smem_addr(a_hi) + (a_off + sl * a_step) * ESZ;
                 const uint32_t d = tmem + d_col + sl * d_step;
                 for (int s = 0; s < nk; ++s) {
-                    const uint32_t step = s * 256;  // two core matrices along K per MMA
-                    const uint64_t ad = sdesc(a0 + step, 128, sbo), gd = sdesc(g0 + step, 128, sbo);
+                    const uint32_t gs = s * 256;  // two core matrices along K per MMA
+                    const uint64_t ad = sdesc(a0 + s * a_kstep, a_lbo, a_sbo), gd = sdesc(g0 + gs, 128, g_sbo);
                     mma<TF>(d, ad, gd, id, s > 0 ? 1u : 0u);
                     if constexpr (MODE == kTcBf16x3) {
-                        mma<TF>(d, ad, sdesc(g0 + G_LO + step, 128, sbo), id, 1u);
-                        mma<TF>(d, sdesc(a0 + A_LO + step, 128, sbo), gd, id, 1u);
+                        mma<TF>(d, ad, sdesc(g0 + G_LO + gs, 128, g_sbo), id, 1u);
+                        mma<TF>(d, sdesc(a0 + A_LO + s * a_kstep, a_lbo, a_sbo), gd, id, 1u);
                     }
                 }
             }
@@ -376,47 +398,69 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc_kernel(const __grid_constan
             }
         }
         handoff();
-        bool ok = gemm(C_D1, 0, B, L::g1, B, B / KSTEP, T, 128 * B, B);  // D1[t] = rows of slice t
+        bool ok = gemm(C_D1, 0, B, false, L::g1, B, B / KSTEP, T, 128 * B, B);  // D1[t] = rows of slice t
         if (!ok) {
             s_fail_any = true;
             break;
         }
 
-        // ---- A2[(blk, kx)][(t, c, y)] from the packed row spectra
+        // ---- A2[t][(blk, kx)][(c, y)] (MN-major) from the packed row spectra: thread (blk, y)
+        //      writes the real (half 0) or imaginary (half 1) parts of its row, kx = 0 .. B-1
         {
             const int blk = row / B, y = row % B;
 #pragma unroll
             for (int t = 0; t < T; ++t) {
+                float v[B];
 #pragma unroll
-                for (int j8 = 0; j8 < B / 16; ++j8) {
-                    const int jb = half * (B / 2) + j8 * 8;
-                    float v[8];
-                    tmem_ld8(tmem + lane_base + C_D1 + t * B + jb, v);
-                    tmem_wait_ld();
+                for (int j8 = 0; j8 < B / 8; ++j8) {
+                    float w8[8];
+                    tmem_ld8(tmem + lane_base + C_D1 + t * B + j8 * 8, w8);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) v[j8 * 8 + i] = w8[i];
+                }
+                tmem_wait_ld();
+                char* base = a_hi + (size_t)t * 128 * 2 * B * ESZ;
+#pragma unroll
+                for (int q = 0; q < B / 8; ++q) {  // kx = 8q .. 8q+7
+                    float c8[8];
 #pragma unroll
                     for (int i = 0; i < 8; ++i) {
-                        const int j = jb + i;
-                        const int kx = j == 0 ? 0 : (j == 1 ? B / 2 : j >> 1);
-                        const int c = j < 2 ? 0 : (j & 1);
-                        put<MODE>(a_hi, A_LO, op_index<ESZ>(blk * B + kx, (t * 2 + c) * B + y, K2), v[i]);
-                        if (j < 2) put<MODE>(a_hi, A_LO, op_index<ESZ>(blk * B + kx, (t * 2 + 1) * B + y, K2), 0.0f);
+                        const int kx = 8 * q + i;
+                        float re = 0.0f, im = 0.0f;
+                        if (kx == 0) re = v[0];
+                        else if (kx == B / 2) re = v[1];
+                        else if (kx < B / 2) { re = v[2 * kx]; im = v[2 * kx + 1]; }
+                        c8[i] = half ? im : re;
+                    }
+                    if constexpr (TF) {  // tf32 operands stay K-major (MN-major is for 16-bit types)
+#pragma unroll
+                        for (int i = 0; i < 8; ++i)
+                            put<MODE>(base, A_LO, op_index<ESZ>(blk * B + 8 * q + i, half * B + y, 2 * B), c8[i]);
+                    } else {
+                        put8_mn<MODE>(base, A_LO, blk * B + 8 * q, half * B + y, c8);
                     }
                 }
             }
         }
         handoff();
-        ok = gemm(C_D2, 0, K2, L::g2, K2, K2 / KSTEP);
+        ok = gemm(C_D2, 0, 2 * B, !TF, L::g2, 2 * B, 2 * B / KSTEP, T, 128 * 2 * B, 2 * B);
         if (!ok) {
             s_fail_any = true;
             break;
         }
 
-        // ---- zero-mean, gain, temporal inverse of the centre frame -> A4[(blk, kx)][(c, ky)]
+        // ---- temporal DFT, zero-mean, gain, temporal inverse of the centre frame -> A4[(blk, kx)][(c, ky)]
         {
             const int blk = row / B, kx = row % B;
-            float z00;
-            tmem_ld1(tmem + lane_base + C_D2, z00);  // Re Z(kt 0, ky 0) of this row
-            tmem_wait_ld();
+            // Re Z(kt 0, ky 0) of this row = sum over t of the column products at (c 0, ky 0)
+            float z00 = 0.0f;
+#pragma unroll
+            for (int t = 0; t < T; ++t) {
+                float z;
+                tmem_ld1(tmem + lane_base + C_D2 + t * 2 * B, z);
+                tmem_wait_ld();
+                z00 += z;
+            }
             const float dc = __shfl_sync(0xffffffffu, z00, (tid & 31) & ~(B - 1) & 31);
             const float g = P.g_div != 0.0f ? __fdiv_rn(dc, P.g_div) : 0.0f;
             // tensor-memory loads are warp-wide: every lane loads, rows kx > B/2 and blocks past the tile end discard
@@ -425,30 +469,40 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc_kernel(const __grid_constan
 #pragma unroll
             for (int k8 = 0; k8 < B / 16; ++k8) {
                 const int kb = half * (B / 2) + k8 * 8;
+                float pr[T][8], pi[T][8];
+#pragma unroll
+                for (int t = 0; t < T; ++t) {
+                    tmem_ld8(tmem + lane_base + C_D2 + t * 2 * B + kb, pr[t]);
+                    tmem_ld8(tmem + lane_base + C_D2 + t * 2 * B + B + kb, pi[t]);
+                }
+                tmem_wait_ld();
                 float yr[8], yi[8];
 #pragma unroll
-                for (int i = 0; i < 8; ++i) yr[i] = yi[i] = 0.0f;
+                for (int i = 0; i < 8; ++i) {
+                    float re[T], im[T];
 #pragma unroll
-                for (int kt = 0; kt < T; ++kt) {
-                    float zr[8], zi[8];
-                    tmem_ld8(tmem + lane_base + C_D2 + (kt * 2) * B + kb, zr);
-                    tmem_ld8(tmem + lane_base + C_D2 + (kt * 2 + 1) * B + kb, zi);
-                    tmem_wait_ld();
-                    // e^{+2 pi i kt r / T}
-                    float sn, cs;
-                    sincospif(2.0f * (float)((kt * R) % T) / (float)T, &sn, &cs);
+                    for (int t = 0; t < T; ++t) {
+                        re[t] = pr[t][i];
+                        im[t] = pi[t][i];
+                    }
+                    if constexpr (T > 1) cdft_n<T>(re, im, false);
+                    float sr = 0.0f, si = 0.0f;
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) {
+                    for (int kt = 0; kt < T; ++kt) {
                         const int tb = (kxc * T + kt) * B + kb + i;
                         const float wr = s_wf[2 * tb], wi = s_wf[2 * tb + 1];
-                        const float dre = fmaf(-g, wr, zr[i]), dim = fmaf(-g, wi, zi[i]);
+                        const float dre = fmaf(-g, wr, re[kt]), dim = fmaf(-g, wi, im[kt]);
                         const float psd = fmaf(dim, dim, dre * dre);
                         const float s = s_sig[tb];
                         const float m = FC == kFilterWiener ? gain<0>(psd, s, P) : gain_rt(P.filter_type, psd, s, P);
                         const float ur = fmaf(m, dre, g * wr), ui = fmaf(m, dim, g * wi);
-                        yr[i] += ur * cs - ui * sn;
-                        yi[i] += ur * sn + ui * cs;
+                        // e^{+2 pi i kt r / T}
+                        const float cs = CentreTwiddle<T>::re(kt), sn = CentreTwiddle<T>::im(kt);
+                        sr += ur * cs - ui * sn;
+                        si += ur * sn + ui * cs;
                     }
+                    yr[i] = sr;
+                    yi[i] = si;
                 }
                 if (active) {
                     put8<MODE>(a_hi, A_LO, op_index<ESZ>(row, kb, 2 * B), yr);
@@ -457,40 +511,40 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc_kernel(const __grid_constan
             }
         }
         handoff();
-        ok = gemm(C_D4, 0, 2 * B, L::g4, 2 * B, 2 * B / KSTEP);
+        ok = gemm(C_D4, 0, 2 * B, false, L::g4, 2 * B, 2 * B / KSTEP);
         if (!ok) {
             s_fail_any = true;
             break;
         }
 
-        // ---- A5[(blk, y)][j]: inverse column outputs repacked for c2r
+        // ---- A5[(blk, y)][j] (MN-major): thread (blk, kx) writes its y-half of columns j(kx, re / im)
         {
             const int blk = row / B, kx = row % B;
-            float vr[B / 2], vi[B / 2];
 #pragma unroll
             for (int y8 = 0; y8 < B / 16; ++y8) {
-                float t0[8], t1[8];
-                tmem_ld8(tmem + lane_base + C_D4 + half * (B / 2) + y8 * 8, t0);
-                tmem_ld8(tmem + lane_base + C_D4 + B + half * (B / 2) + y8 * 8, t1);
+                const int yb = half * (B / 2) + y8 * 8;
+                float vr[8], vi[8];
+                tmem_ld8(tmem + lane_base + C_D4 + yb, vr);
+                tmem_ld8(tmem + lane_base + C_D4 + B + yb, vi);
                 tmem_wait_ld();
+                if (kx <= B / 2) {
+                    const int jr = kx == 0 ? 0 : (kx == B / 2 ? 1 : 2 * kx);
+                    const bool pair = kx != 0 && kx != B / 2;
+                    if constexpr (TF) {
 #pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    vr[y8 * 8 + i] = t0[i];
-                    vi[y8 * 8 + i] = t1[i];
-                }
-            }
-            if (kx <= B / 2) {
-                const int jr = kx == 0 ? 0 : (kx == B / 2 ? 1 : 2 * kx);
-#pragma unroll
-                for (int i = 0; i < B / 2; ++i) {
-                    const int y = half * (B / 2) + i;
-                    put<MODE>(a_hi, A_LO, op_index<ESZ>(blk * B + y, jr, B), vr[i]);
-                    if (kx != 0 && kx != B / 2) put<MODE>(a_hi, A_LO, op_index<ESZ>(blk * B + y, jr + 1, B), vi[i]);
+                        for (int i = 0; i < 8; ++i) {
+                            put<MODE>(a_hi, A_LO, op_index<ESZ>(blk * B + yb + i, jr, B), vr[i]);
+                            if (pair) put<MODE>(a_hi, A_LO, op_index<ESZ>(blk * B + yb + i, jr + 1, B), vi[i]);
+                        }
+                    } else {
+                        put8_mn<MODE>(a_hi, A_LO, blk * B + yb, jr, vr);
+                        if (pair) put8_mn<MODE>(a_hi, A_LO, blk * B + yb, jr + 1, vi);
+                    }
                 }
             }
         }
         handoff();
-        ok = gemm(C_D5, 0, B, L::g5, B, B / KSTEP);
+        ok = gemm(C_D5, 0, B, !TF, L::g5, B, B / KSTEP);
         if (!ok) {
             s_fail_any = true;
             break;

@@ -69,6 +69,21 @@ class GradPlane(ctypes.Structure):
     ]
 
 
+class HostPlane(ctypes.Structure):
+    """dfttest2_b200_host_plane: one plane of a clip in host memory."""
+
+    _fields_ = [
+        ("src", c_void_p),
+        ("src_stride", c_ssize_t),
+        ("src_frame_bytes", c_ssize_t),
+        ("dst", c_void_p),
+        ("dst_stride", c_ssize_t),
+        ("dst_frame_bytes", c_ssize_t),
+        ("width", c_int),
+        ("height", c_int),
+    ]
+
+
 class Clip(ctypes.Structure):
     """dfttest2_b200_clip: one device-resident clip of a multi-clip batch."""
 
@@ -104,6 +119,7 @@ SIGNATURES = {
         c_int,
         [c_void_p, c_void_p, c_ssize_t, c_ssize_t, c_void_p, c_ssize_t, c_ssize_t, c_int, c_int, c_int, c_int, c_int],
     ),
+    "dfttest2_b200_process_clip_planes_host": (c_int, [c_void_p, POINTER(HostPlane), c_int, c_int, c_int, c_int]),
     "dfttest2_b200_process_planes_sigma": (c_int, [c_void_p, POINTER(Plane), c_int, c_int, c_int, c_void_p, c_void_p]),
     "dfttest2_b200_backward_planes": (c_int, [c_void_p, POINTER(GradPlane), c_int, c_void_p, c_void_p, c_void_p]),
     "dfttest2_b200_set_precision": (c_int, [c_void_p, c_int]),

@@ -112,6 +112,23 @@ class Filter:
             out.strides[0], n, w, h, sample_type, bits))
         return out
 
+    def process_clip_planes_host(self, planes: Sequence[np.ndarray], sample_type: int, bits: int) -> list:
+        """All frames of several planes of one clip (each an (N, H_i, W_i) host
+        array, same N and sample format) through one host pipeline."""
+        planes = [np.ascontiguousarray(p) for p in planes]
+        n = planes[0].shape[0]
+        if any(p.shape[0] != n for p in planes):
+            raise Error("all planes need the same number of frames")
+        outs = [np.empty_like(p) for p in planes]
+        arr = (_lib.HostPlane * len(planes))()
+        for a, p, o in zip(arr, planes, outs):
+            a.src, a.src_stride, a.src_frame_bytes = p.ctypes.data, p.strides[1], p.strides[0]
+            a.dst, a.dst_stride, a.dst_frame_bytes = o.ctypes.data, o.strides[1], o.strides[0]
+            a.width, a.height = p.shape[2], p.shape[1]
+        _lib.check(self._lib.dfttest2_b200_process_clip_planes_host(self.handle, arr, len(planes), n, sample_type,
+                                                                    bits))
+        return outs
+
     def process_planes_device(self, planes: Sequence[dict], sample_type: int, bits: int, stream: int = 0) -> None:
         """Device pointers; each dict has src (list of 2r+1 pointers), src_stride,
         dst, dst_stride, width, height (strides in bytes).  Asynchronous."""
@@ -174,15 +191,16 @@ class _Plugin:
         flt = Filter(window, sigma, sigma2, pmin, pmax, filter_type, radius, block_size, block_step, zero_mean,
                      window_freq, device_id, num_streams, synthesis_slice)
         try:
-            out = []
-            for p in range(fmt.num_planes):
-                src = clip.planes[p]
-                if not process[p]:
-                    out.append(src)
-                elif clip.on_gpu:
-                    out.append(flt.process_clip_device(src, fmt.sample_type, fmt.bits_per_sample))
-                else:
-                    out.append(flt.process_clip_host(src, fmt.sample_type, fmt.bits_per_sample))
+            out = list(clip.planes)
+            todo = [p for p in range(fmt.num_planes) if process[p]]
+            if clip.on_gpu:
+                for p in todo:
+                    out[p] = flt.process_clip_device(clip.planes[p], fmt.sample_type, fmt.bits_per_sample)
+            elif todo:
+                # every processed plane through one host pipeline
+                for p, o in zip(todo, flt.process_clip_planes_host([clip.planes[p] for p in todo], fmt.sample_type,
+                                                                   fmt.bits_per_sample)):
+                    out[p] = o
             if clip.on_gpu:
                 import torch
 
