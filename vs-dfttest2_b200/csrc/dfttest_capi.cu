@@ -622,6 +622,16 @@ struct DeviceGuard {
     }
 };
 
+// Window-spectrum entry (re, im) of temporal bin t as the FP32 kernel sees
+// it: the kernel feeds each block's frames centre first (frame r at time 0),
+// which multiplies temporal bin t of every spectrum by w^(t r), w = e^(2 pi i / T).
+void centre_first_wf(const double* wf, int t, int T, int r, float& re, float& im) {
+    const double ang = 2.0 * 3.14159265358979323846 * (double)((t * r) % T) / T;
+    const double c = std::cos(ang), sn = std::sin(ang);
+    re = (float)(wf[0] * c - wf[1] * sn);
+    im = (float)(wf[0] * sn + wf[1] * c);
+}
+
 void scale_peak(int sample_type, int bits, float& scale, float& peak, int& kind) {
     if (sample_type == DFTTEST2_B200_FLOAT) {
         scale = 255.0f;
@@ -787,9 +797,9 @@ int dfttest2_b200_create(const dfttest2_b200_params* p, dfttest2_b200_filter** o
     auto sigma_at = [&](int t, int y, int x) -> float {
         return p->sigma_len == 1 ? (float)p->sigma[0] : (float)p->sigma[(t * B + y) * X + x];
     };
-    auto wf_at = [&](int t, int y, int x, int part) -> float {
-        if (!zero_mean) return 0.0f;
-        return (float)p->window_freq[((t * B + y) * X + x) * 2 + part];
+    auto wf_rot = [&](int t, int y, int x, float& re, float& im) {
+        re = im = 0.0f;
+        if (zero_mean) centre_first_wf(&p->window_freq[((t * B + y) * X + x) * 2], t, T, radius, re, im);
     };
     // Gain-slot tables, laid out [plane][slot][lane w = 2c + h] as the column
     // phase reads them: lane (c, h) holds the y-bins k = 2m + h of packed
@@ -805,8 +815,7 @@ int dfttest2_b200_create(const dfttest2_b200_params* p, dfttest2_b200_filter** o
         sig2_idx[idx] = (t2 * B + y2) * X + x;
         sig[idx] = sigma_at(t, y, x);
         sig2[idx] = sigma_at(t2, y2, x);
-        wfe[2 * idx] = wf_at(t, y, x, 0);
-        wfe[2 * idx + 1] = wf_at(t, y, x, 1);
+        wf_rot(t, y, x, wfe[2 * idx], wfe[2 * idx + 1]);
         if (sig2[idx] != sig[idx]) asym = true;
     };
     auto neg = [&](int k) { return (B - k) % B; };
@@ -876,8 +885,9 @@ int dfttest2_b200_create(const dfttest2_b200_params* p, dfttest2_b200_filter** o
                 for (int x = 0; x < X; ++x) {
                     const int i = (t * B + y) * X + x;
                     sfull[i] = sigma_at(t, y, x);
-                    wffull[2 * i] = wf_at(t, y, x, 0);
-                    wffull[2 * i + 1] = wf_at(t, y, x, 1);
+                    // natural frame order (the adjoint and tensor-core kernels)
+                    wffull[2 * i] = zero_mean ? (float)p->window_freq[2 * i] : 0.0f;
+                    wffull[2 * i + 1] = zero_mean ? (float)p->window_freq[2 * i + 1] : 0.0f;
                 }
         if (int rc = upload(f->d_sigma_full, sfull)) return rc;
         if (int rc = upload(f->d_wf_full, wffull)) return rc;
@@ -1351,16 +1361,16 @@ extern "C" int dfttest2_b200_process_plane_noalloc(const dfttest2_b200_params* p
     auto sigma_at = [&](int t, int y, int x) -> float {
         return p->sigma_len == 1 ? (float)p->sigma[0] : (float)p->sigma[(t * B + y) * X + x];
     };
-    auto wf_at = [&](int t, int y, int x, int part) -> float {
-        return zero_mean ? (float)p->window_freq[((t * B + y) * X + x) * 2 + part] : 0.0f;
+    auto wf_rot = [&](int t, int y, int x, float& re, float& im) {
+        re = im = 0.0f;
+        if (zero_mean) centre_first_wf(&p->window_freq[((t * B + y) * X + x) * 2], t, T, radius, re, im);
     };
     bool asym = false;
     auto put = [&](int pl, int j, int w, int t, int y, int x, int t2, int y2) {
         const int idx = (pl * NS + j) * B + w;
         tb.sig[idx] = sigma_at(t, y, x);
         tb.sig2[idx] = sigma_at(t2, y2, x);
-        tb.wfe[2 * idx] = wf_at(t, y, x, 0);
-        tb.wfe[2 * idx + 1] = wf_at(t, y, x, 1);
+        wf_rot(t, y, x, tb.wfe[2 * idx], tb.wfe[2 * idx + 1]);
         if (tb.sig2[idx] != tb.sig[idx]) asym = true;
     };
     auto neg = [&](int k) { return (B - k) % B; };

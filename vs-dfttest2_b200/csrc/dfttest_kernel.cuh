@@ -181,11 +181,13 @@ __device__ __forceinline__ float rcp_approx(float x) {
 
 // multiplier of frequency_filtering (cpu_source/kernel.hpp:1826-1890).
 // FT 0 is the Wiener gain max((psd - s) / (psd + 1e-15), 0), evaluated as
-// max(1 - s * rcp(psd + 1e-15), 0); the other types keep IEEE division.
+// max(1 - s * rcp(psd), 0): the 1e-15 only keeps the reference's division
+// finite at psd = 0, where rcp gives +inf and the gain is 0 either way
+// (fmaxf drops the NaN of 0 * inf); the other types keep IEEE division.
 template <int FT>
 __device__ __forceinline__ float gain(float psd, float s, const FilterParams& a) {
     if constexpr (FT == 0) {
-        return fmaxf(fmaf(-s, rcp_approx(psd + 1e-15f), 1.0f), 0.0f);
+        return fmaxf(fmaf(-s, rcp_approx(psd), 1.0f), 0.0f);
     } else if constexpr (FT == 1) {
         return psd < s ? 0.0f : 1.0f;
     } else if constexpr (FT == 2) {
@@ -297,10 +299,14 @@ __device__ __forceinline__ float row_task(float* __restrict__ wb, const float* _
     constexpr int H = B / 2;
     constexpr int R = (T - 1) / 2;
     float X[T][B];
+    // frames in centre-first order (t' = 0 is frame r): the temporal DFT of the
+    // shifted sequence is w^(p r) times that of the original, which is the
+    // centre-frame weight of the inverse, so the inverse becomes a plain sum
 #pragma unroll
     for (int t = 0; t < T; ++t) {
-        const float* src = ring + (t * B + slot_y) * pitch + xoff;
-        const float* w = win + (t * B + y) * TL::WP;
+        const int ft = (t + R) % T;
+        const float* src = ring + (ft * B + slot_y) * pitch + xoff;
+        const float* w = win + (ft * B + y) * TL::WP;
         float v[B];
         if (vec) {
 #pragma unroll
@@ -502,17 +508,15 @@ __device__ __forceinline__ void column_task(float* __restrict__ wb, float g, con
         load_half(wb + p * B * B);
         gain_lane<M, B, FC>(qr, qi, sm_sig + p * NS * B, sm_sig2 + p * NS * B, sm_wfe + 2 * p * NS * B, w, g, dual,
                             (a.wmask >> p) & 1, a);
-        // twiddle w^(p r); the packed lane on a B-column plane uses i * conj(w^(p r))
-        const float tc = CentreTwiddle<T>::re(p), ts = CentreTwiddle<T>::im(p);
-        const bool swap = packed && (p > R);
-        const float twr = swap ? ts : tc;
-        const float twi = swap ? tc : ts;
+        // the centre-frame weight w^(p r) is already in the spectrum (centre-first
+        // frame order); the packed lane enters a B-column plane multiplied by i
+        if (packed && p > R) {
 #pragma unroll
-        for (int k = 0; k < M; ++k) {
-            const float vr = fmaf(qr[k], twr, -qi[k] * twi);
-            const float vi = fmaf(qr[k], twi, qi[k] * twr);
-            qr[k] = vr;
-            qi[k] = vi;
+            for (int k = 0; k < M; ++k) {
+                const float vr = -qi[k];
+                qi[k] = qr[k];
+                qr[k] = vr;
+            }
         }
         if (packed) {
             // Hermitian part (A planes) or anti-Hermitian part (i * B planes)
