@@ -204,7 +204,7 @@ def test_batch_of_planes_matches_single_launches(cuda_device):
 @pytest.mark.parametrize("nframes", [1, 3, 13, 40])
 def test_multi_plane_host_pipeline_equals_device_path(nframes, cuda_device):
     """dfttest2_b200_process_clip_planes_host (one pipeline over the three
-    planes of a YUV420P16 clip, chunks ramping 4, 8, 16, ..., 8, 4) gives the
+    planes of a YUV420P16 clip, chunks ramping 4, 12, 32, ..., 12, 4) gives the
     device path's result for every frame, including the clip-end clamp
     (within 1 LSB: the launches split planes into units differently, which
     reorders the overlap-add sums at unit edges)."""

@@ -1027,24 +1027,24 @@ int dfttest2_b200_process_clip_planes_host(dfttest2_b200_filter* f, const dfttes
     const int r = f->radius;
     SlotGuard sg(f);
     Slot& s = sg.slot();
-    // Chunks of output frames ramp up (4, 8, 16, ...) and down at the end so
+    // Chunks of output frames ramp up (4, 12, 32, ...) and down at the end so
     // that the first upload and the last download, which nothing overlaps,
     // stay short.  Uploads (stream `up`), filtering of every plane's frames of
     // a chunk in one launch (slot stream) and downloads (stream `down`) of
     // consecutive chunks overlap; every source frame is uploaded once into a
     // dense device array; outputs alternate between two chunk buffers.
-    constexpr int kMaxChunk = 16;
+    constexpr int kMaxChunk = 32;
     std::vector<int> chunks;
     {
         int left = nframes;
-        for (int c : {4, 8}) {
+        for (int c : {4, 12}) {
             if (left <= 0) break;
             const int take = std::min(c, left);
             chunks.push_back(take);
             left -= take;
         }
         std::vector<int> tail;
-        for (int c : {4, 8}) {  // the last chunks, smallest last
+        for (int c : {4, 12}) {  // the last chunks, smallest last
             if (left <= 0) break;
             const int take = std::min(c, left);
             tail.push_back(take);
