@@ -45,7 +45,7 @@ FLOP_PER_BLOCK = {1: 9473, 3: 26385, 5: 47329, 7: 74033}  # B = 16, reference co
 METRIC = "1080p YUV420P16 frames/s (DFTTest sbsize16 sosize12 tbsize3, all planes)"
 # DRAM bytes (read + write) of the unit kernel per 1080p YUV420P16 frame, from one ncu capture of a
 # 24-frame launch (profiles/dfttest_unit_16x3_yuv420p16.md); traffic grows with the frames processed
-DRAM_BYTES_PER_FRAME = 17_790_347
+DRAM_BYTES_PER_FRAME = 20_089_600
 
 
 def workload_args():
@@ -519,6 +519,13 @@ def main():
     e2e_frames = world * (in_hi - in_lo) * opts.e2e_steps
     bytes_in = sum(p.nbytes for p in host_planes)
 
+    # kernels per step: the unit kernel, plus the fix-up kernel unless every unit is a
+    # full-height strip (strips of 16 blocks reach 4 x SMs units), when seams are summed in-kernel
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    pn = [(n + ((16 - n % 16) if n % 16 else 0) + 24 - 16) // 4 + 1 for n in (W, W // 2)]
+    strips = (hi - lo) * ((pn[0] + 15) // 16 + 2 * ((pn[1] + 15) // 16))
+    launches_per_step = 1 if strips >= 4 * sms else 2
+
     # ---- roofline
     blocks = blocks_per_frame() * (hi - lo)
     flops_step = blocks * FLOP_PER_BLOCK[2 * r + 1]
@@ -533,7 +540,7 @@ def main():
         "config": workload_config(hi - lo, world, bytes_in),
         "e2e": {"value": e2e_frames / e2e_s, "unit": "frames/s", "h2d_bytes_per_step": bytes_in,
                 "d2h_bytes_per_step": bytes_in, "path": "dfttest2_b200_process_clip_planes_host (3 planes, one pipeline), pinned host memory"},
-        "gpu_launches": 2 * opts.steps,
+        "gpu_launches": launches_per_step * opts.steps,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": DRAM_BYTES_PER_FRAME * (hi - lo),
                      "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum per launch, scaled from a 24-frame "

@@ -151,6 +151,8 @@ struct Slot {
     size_t jobs_cap = 0;
     float* d_scratch = nullptr;
     size_t scratch_cap = 0;               // floats
+    int* d_seams = nullptr;               // seam arrival counters (full-strip launches)
+    size_t seams_cap = 0;
     int* d_error = nullptr;
     // host path staging
     void* d_frames = nullptr;
@@ -291,6 +293,8 @@ struct Plan {
     int nfix = 0;
     int rec_stride = 0;
     int pitch = 0;
+    int nseams = 0;            // seams between strips, summed over jobs
+    bool full_strips = false;  // every job has nsy = 1
 };
 
 // a plane in the work-list: strides in elements, `param` indexes per-job formats and filters
@@ -321,7 +325,8 @@ void plan_units(int B, int S, int BPS, const std::vector<PlaneRef>& planes, long
     const int min_seg = std::max((O + S - 1) / S, 4);
     nsy = std::max(1, std::min(nsy, max_pny / min_seg));
 
-    int unit = 0, fix = 0, rec = 0;
+    int unit = 0, fix = 0, rec = 0, seams = 0;
+    bool full = true;
     for (int i = 0; i < n; ++i) {
         const PlaneRef& p = planes[i];
         dft2::PlaneJob& j = plan.jobs[i];
@@ -340,6 +345,9 @@ void plan_units(int B, int S, int BPS, const std::vector<PlaneRef>& planes, long
         while (j.nsx > 1 && pnx / j.nsx < (O + S - 1) / S) --j.nsx;
         j.unit_base = unit;
         j.fix_base = fix;
+        j.seam_base = seams;
+        seams += j.nsx - 1;
+        full = full && j.nsy == 1;
         unit += j.nsx * j.nsy;
         fix += (j.nsx - 1) * O * p.height + (j.nsy - 1) * O * p.width;
         const int wmax = (pnx + j.nsx - 1) / j.nsx, hmax = (pny + j.nsy - 1) / j.nsy;
@@ -349,6 +357,8 @@ void plan_units(int B, int S, int BPS, const std::vector<PlaneRef>& planes, long
     plan.nfix = fix;
     plan.rec_stride = std::max(rec, 1);
     plan.pitch = ((BPS * S + O) + 3) & ~3;
+    plan.nseams = seams;
+    plan.full_strips = full;
 }
 
 // the mirror padding must stay inside the plane (cpu_source/getframe_impl.cpp:44-62 reads 2*ox - x)
@@ -595,13 +605,20 @@ int launch(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, floa
     a.rec_stride = plan.rec_stride;
     a.ring_pitch = plan.pitch;
     a.error_flag = slot.d_error;
+    // full-height strips: the unit kernel sums its seams itself
+    const bool inline_seams = plan.nfix > 0 && plan.full_strips && plan.nseams > 0;
+    if (inline_seams) {
+        if (int rc = ensure(slot.d_seams, slot.seams_cap, (size_t)plan.nseams, slot.done)) return rc;
+        CUDA_TRY(cudaMemsetAsync(slot.d_seams, 0, (size_t)plan.nseams * sizeof(int), stream));
+        a.seam_count = slot.d_seams;
+    }
 
     const size_t smem = f->var.smem(plan.pitch);
     KernelFn kern = (f->filter_type == 0 && !f->asym && !sig_override) ? f->var.main : f->var.generic;
     CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<plan.nunits, f->var.nw * 32, smem, stream>>>(a);
     CUDA_TRY(cudaGetLastError());
-    if (plan.nfix > 0) {
+    if (plan.nfix > 0 && !inline_seams) {
         const int threads = 256;
         const int blocks = std::min((plan.nfix + threads - 1) / threads, f->num_sms * 8);
         f->var.fixup<<<blocks, threads, 0, stream>>>(a);
@@ -697,6 +714,7 @@ void free_filter(dfttest2_b200_filter* f) {
         if (s.done) cudaEventSynchronize(s.done);
         if (s.d_jobs) cudaFree(s.d_jobs);
         if (s.d_scratch) cudaFree(s.d_scratch);
+        if (s.d_seams) cudaFree(s.d_seams);
         if (s.d_error) cudaFree(s.d_error);
         if (s.d_frames) cudaFree(s.d_frames);
         if (s.d_sigtab) cudaFree(s.d_sigtab);

@@ -57,7 +57,7 @@ struct PlaneJob {
     int unit_base;        // first global unit id of this job
     int fix_base;         // first global fix-up pixel id of this job
     int param;            // index into KernelArgs::params (batched launches)
-    int pad_;
+    int seam_base;        // first seam counter of this job (KernelArgs::seam_count)
 };
 
 // sample format and filter of a plane: launch-wide, or per job in a batch
@@ -89,6 +89,11 @@ struct KernelArgs {
     int rec_stride;    // floats per unit record
     int ring_pitch;    // floats per ring row
     int* error_flag;   // set to a non-zero code on an internal consistency failure
+    // Launches whose units are full-height strips (nsy = 1 for every job): one
+    // arrival counter per seam between neighbouring strips, zeroed before the
+    // launch; the second strip to finish sums the seam, and no fix-up kernel
+    // runs.  Null: the fix-up kernel sums the shared pixels.
+    int* seam_count;
 };
 
 __host__ __device__ inline int pad_size(int n, int B, int S) {
@@ -871,6 +876,40 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
                 const long long sy_ = mirror(py - oy, Hh);
                 const int sxp = min(sx_lo + li * (128 / esz), sx_hi);
                 prefetch_l2(reinterpret_cast<const char*>(job.src[t]) + (sy_ * job.src_stride + sxp) * esz);
+            }
+        }
+    }
+
+    // ---- seams shared with the neighbouring full-height strips: the second of
+    // the two strips to finish sums both band records (left strip first, as
+    // the fix-up kernel does) and stores the result
+    if (a.seam_count != nullptr) {
+        __shared__ int s_arrival;
+        __threadfence();  // this unit's band records are visible before it arrives
+        __syncthreads();
+#pragma unroll 1
+        for (int side = 0; side < 2; ++side) {
+            const int k = side == 0 ? sx - 1 : sx;  // seam k lies between strips k and k + 1
+            if (k < 0 || k >= job.nsx - 1) continue;
+            if (tid == 0) s_arrival = atomicAdd(a.seam_count + job.seam_base + k, 1);
+            __syncthreads();
+            const bool second = (s_arrival == 1);
+            __syncthreads();
+            if (!second) continue;
+            __threadfence();
+            const UnitGeom ul = unit_geom(k, 0, job.nsx, 1, pnx, pny, B, S);
+            const UnitGeom ur = unit_geom(k + 1, 0, job.nsx, 1, pnx, pny, B, S);
+            const float* recl = a.scratch + (size_t)(job.unit_base + k) * a.rec_stride;
+            const float* recr = a.scratch + (size_t)(job.unit_base + k + 1) * a.rec_stride;
+            const int pxs = ur.bx0 * S;  // first padded column of the seam
+            for (int i = tid; i < O * Hh; i += NT) {
+                const int r = i / O;
+                const int py = oy + r, px = pxs + (i - r * O);
+                if (px < ox || px >= ox + W) continue;
+                const float v = 0.0f + __ldcg(recl + band_index(px - ul.bx0 * S, py - ul.by0 * S, ul.fw, ul.fh, O)) +
+                                __ldcg(recr + band_index(px - ur.bx0 * S, py - ur.by0 * S, ur.fw, ur.fh, O));
+                store_sample(job.dst, (long long)(py - oy) * job.dst_stride + (px - ox), v, P.kind, P.scale, P.peak,
+                             is_float ? 0.0f : inv_scale);
             }
         }
     }
