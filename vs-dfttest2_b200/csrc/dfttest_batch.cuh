@@ -23,6 +23,7 @@ struct dfttest2_b200_batch {
         Plan plan;
         dft2::PlaneJob* d_jobs = nullptr;
         float* d_scratch = nullptr;
+        int* d_seams = nullptr;        // seam counters when every unit is a full-height strip
         std::string trials;            // "shape:ms ..." of the tuning runs
         bool cached = false;
     };
@@ -51,6 +52,7 @@ void free_batch(dfttest2_b200_batch* b) {
     for (auto& gr : b->groups) {
         if (gr.d_jobs) cudaFree(gr.d_jobs);
         if (gr.d_scratch) cudaFree(gr.d_scratch);
+        if (gr.d_seams) cudaFree(gr.d_seams);
     }
     for (cudaStream_t s : b->branch) cudaStreamDestroy(s);
     for (cudaEvent_t e : b->ev) cudaEventDestroy(e);
@@ -73,11 +75,15 @@ int launch_group(const dfttest2_b200_batch* b, const dfttest2_b200_batch::Group&
     a.rec_stride = g.plan.rec_stride;
     a.ring_pitch = g.plan.pitch;
     a.error_flag = b->d_error;
+    if (g.d_seams) {  // full-height strips: seams summed in the unit kernel
+        CUDA_TRY(cudaMemsetAsync(g.d_seams, 0, (size_t)g.plan.nseams * sizeof(int), st));
+        a.seam_count = g.d_seams;
+    }
     const size_t smem = var.smem(g.plan.pitch);
     KernelFn kern = g.generic ? var.generic : var.main;
     kern<<<g.plan.nunits, var.nw * 32, smem, st>>>(a);
     CUDA_TRY(cudaGetLastError());
-    if (g.plan.nfix > 0) {
+    if (g.plan.nfix > 0 && !g.d_seams) {
         const int threads = 256;
         const int blocks = std::min((g.plan.nfix + threads - 1) / threads, b->num_sms * 8);
         var.fixup<<<blocks, threads, 0, st>>>(a);
@@ -98,8 +104,12 @@ int prepare_group(dfttest2_b200_batch* b, dfttest2_b200_batch::Group& g, int var
     CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (g.d_jobs) CUDA_TRY(cudaFree(g.d_jobs));
     if (g.d_scratch) CUDA_TRY(cudaFree(g.d_scratch));
+    if (g.d_seams) CUDA_TRY(cudaFree(g.d_seams));
     g.d_jobs = nullptr;
     g.d_scratch = nullptr;
+    g.d_seams = nullptr;
+    if (g.plan.nfix > 0 && g.plan.full_strips && g.plan.nseams > 0)
+        CUDA_TRY(cudaMalloc((void**)&g.d_seams, (size_t)g.plan.nseams * sizeof(int)));
     CUDA_TRY(cudaMalloc((void**)&g.d_jobs, g.plan.jobs.size() * sizeof(dft2::PlaneJob)));
     CUDA_TRY(cudaMalloc((void**)&g.d_scratch, (size_t)g.plan.nunits * g.plan.rec_stride * sizeof(float)));
     CUDA_TRY(cudaMemcpy(g.d_jobs, g.plan.jobs.data(), g.plan.jobs.size() * sizeof(dft2::PlaneJob),
@@ -338,13 +348,13 @@ int dfttest2_b200_batch_describe(const dfttest2_b200_batch* b, char* buf, int le
     for (const auto& g : b->groups) {
         const Variant& v = g.cands[g.var_idx];
         char line[256];
-        std::snprintf(line, sizeof line, "B%d S%d T%d %s: %d warps x %d units, %zu jobs, %lld blocks, fixup %d%s | ",
+        std::snprintf(line, sizeof line, "B%d S%d T%d %s: %d warps x %d units, %zu jobs, %lld blocks, %s %d%s | ",
                       g.B, g.S, g.T, g.generic ? "general" : "wiener", v.nw, g.plan.nunits, g.plan.jobs.size(),
-                      g.blocks, g.plan.nfix, g.cached ? ", cached" : "");
+                      g.blocks, g.d_seams ? "in-kernel seams" : "fixup", g.plan.nfix, g.cached ? ", cached" : "");
         s += line;
         s += g.trials.empty() ? "untuned" : g.trials;
         s += "\n";
-        launches += 1 + (g.plan.nfix > 0 ? 1 : 0);
+        launches += 1 + (g.plan.nfix > 0 && !g.d_seams ? 1 : 0);
     }
     if (buf && len > 0) {
         const size_t n = std::min(s.size(), (size_t)len - 1);
