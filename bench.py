@@ -375,6 +375,8 @@ def main():
     ap.add_argument("--workload", default="yuv1080p", choices=["yuv1080p", "batch"],
                     help="batch: the 32-clip multi-clip batching workload (one GPU)")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--fbf-frames", type=int, default=32,
+                    help="frames filtered frame by frame through the cached per-plane host path (0 skips)")
     ap.add_argument("--tc-steps", type=int, default=10,
                     help="steps timed for each tensor-core precision mode (0 skips the comparison)")
     opts = ap.parse_args()
@@ -526,6 +528,52 @@ def main():
     strips = (hi - lo) * ((pn[0] + 15) // 16 + 2 * ((pn[1] + 15) // 16))
     launches_per_step = 1 if strips >= 4 * sms else 2
 
+    # ---- frame by frame, as a VapourSynth GetFrame drives the library: one cached per-plane
+    # host call per plane of each output frame, source planes cached on the device by frame number
+    fbf = {}
+    nfb = min(opts.fbf_frames, in_hi - in_lo)
+    if nfb > 0 and world == 1:
+        import ctypes
+        from concurrent.futures import ThreadPoolExecutor
+
+        fbf_flt = Filter(device_id=local, num_streams=4, **args)
+        reqs = []
+        for n in range(nfb):
+            for p in range(3):
+                src = host_planes[p]
+                N, ph, pw = src.shape
+                pl = _lib.Plane()
+                ids = [min(max(n - r + t, 0), N - 1) for t in range(2 * r + 1)]
+                for t, k in enumerate(ids):
+                    pl.src[t] = src[k].ctypes.data
+                out = np.empty((ph, pw), src.dtype)
+                pl.src_stride = pw * 2
+                pl.dst = out.ctypes.data
+                pl.dst_stride = pw * 2
+                pl.width, pl.height = pw, ph
+                reqs.append((n, pl, (ctypes.c_int * len(ids))(*ids), p, out))
+
+        def frame(n):
+            for rn, pl, ids, p, _ in reqs[3 * n:3 * n + 3]:
+                rc = lib.dfttest2_b200_process_plane_host_cached(fbf_flt.handle, ctypes.byref(pl), ids, p, 0, 16)
+                if rc:
+                    return lib.dfttest2_b200_last_error().decode()
+            return ""
+
+        for threads in (1, 4):
+            with ThreadPoolExecutor(threads) as pool:
+                list(pool.map(frame, range(min(nfb, 8))))  # warm-up (allocations)
+                t0 = time.perf_counter()
+                errs = [e for e in pool.map(frame, range(nfb)) if e]
+                dt = time.perf_counter() - t0
+            if errs:
+                raise RuntimeError(errs[0])
+            fbf[f"threads_{threads}"] = nfb / dt
+        fbf_flt.close()
+        fbf = {"value_by_threads": fbf, "unit": "frames/s", "frames": nfb,
+               "path": "dfttest2_b200_process_plane_host_cached per plane per frame (pageable host frames), "
+                       "source planes cached on the device by frame number"}
+
     # ---- roofline
     blocks = blocks_per_frame() * (hi - lo)
     flops_step = blocks * FLOP_PER_BLOCK[2 * r + 1]
@@ -551,6 +599,7 @@ def main():
                      "hbm_peak_gbs": measured_peaks().get("hbm_gbs")},
         "clocks": clocks.summary(),
         "tc": tc_results,
+        "e2e_frame_by_frame": fbf or None,
     }
     if world == 1 and rank == 0 and not opts.no_cpu_baseline:
         result["cpu_baseline"] = cpu_reference_fps(args, host_planes)

@@ -112,6 +112,19 @@ int dfttest2_b200_process_planes(dfttest2_b200_filter* f, const dfttest2_b200_pl
 int dfttest2_b200_process_plane_host(dfttest2_b200_filter* f, const dfttest2_b200_plane* plane, int sample_type,
                                      int bits_per_sample);
 
+/* As dfttest2_b200_process_plane_host, for hosts that filter a clip frame by
+ * frame (a VapourSynth GetFrame): src_frame_ids[t] is the clip frame number of
+ * plane->src[t] (after the clip-end clamp) and plane_index the plane of the
+ * format.  Source planes are kept on the device keyed by (frame number,
+ * plane index), so consecutive frames upload each source frame once instead
+ * of 2r+1 times (the reference uploads a padded stack of 2r+1 frames per
+ * output frame, nvrtc_source/source.cpp:456-551).  The key must identify the
+ * plane's contents for the life of the filter (true for the frames of one
+ * clip).  Thread-safe; at most 64 planes are cached per filter. */
+int dfttest2_b200_process_plane_host_cached(dfttest2_b200_filter* f, const dfttest2_b200_plane* plane,
+                                            const int* src_frame_ids, int plane_index, int sample_type,
+                                            int bits_per_sample);
+
 /* Whole-clip host path: filters `nframes` frames of one plane stored
  * contiguously in host memory (frame i at src + i*frame_bytes, rows
  * src_stride bytes apart) into dst.  Each source frame is uploaded once

@@ -204,6 +204,22 @@ struct dfttest2_b200_filter {
     std::vector<int> free_slots;
     std::mutex slot_lock;
     std::condition_variable slot_cv;
+
+    // source planes already on the device, keyed by (clip frame number, plane
+    // index), for the per-frame host path (dfttest2_b200_process_plane_host_cached)
+    struct CacheEntry {
+        int id = -1, plane = -1;
+        size_t bytes = 0, cap = 0;
+        void* d = nullptr;
+        int refs = 0;                   // calls using the entry
+        bool issued = false;            // its upload is queued (`ready` recorded)
+        unsigned long long used = 0;    // last use, for least-recently-used eviction
+        cudaEvent_t ready = nullptr;
+    };
+    std::vector<CacheEntry> cache;
+    std::mutex cache_lock;
+    std::condition_variable cache_cv;
+    unsigned long long cache_clock = 0;
 };
 
 namespace {
@@ -710,6 +726,10 @@ int launch_adjoint(int B, int T, const dft2::AdjointArgs& a, int num_sms, cudaSt
 void free_filter(dfttest2_b200_filter* f) {
     if (!f) return;
     DeviceGuard g(f->device);
+    for (auto& e : f->cache) {
+        if (e.d) cudaFree(e.d);
+        if (e.ready) cudaEventDestroy(e.ready);
+    }
     for (Slot& s : f->slots) {
         if (s.done) cudaEventSynchronize(s.done);
         if (s.d_jobs) cudaFree(s.d_jobs);
@@ -914,6 +934,7 @@ int dfttest2_b200_create(const dfttest2_b200_params* p, dfttest2_b200_filter** o
         f->n_slots = T * NS * B;
     }
 
+    f->cache.reserve(64);  // entries are referenced outside the lock: never reallocate
     f->slots.resize(num_streams);
     for (int i = 0; i < num_streams; ++i) {
         Slot& s = f->slots[i];
@@ -1022,6 +1043,147 @@ int dfttest2_b200_process_plane_host(dfttest2_b200_filter* f, const dfttest2_b20
     uint8_t* dst = (uint8_t*)plane->dst;
     for (int y = 0; y < plane->height; ++y) std::memcpy(dst + y * plane->dst_stride, h + T * frame + y * row, row);
     return 0;
+}
+
+int dfttest2_b200_process_plane_host_cached(dfttest2_b200_filter* f, const dfttest2_b200_plane* plane,
+                                            const int* src_frame_ids, int plane_index, int sample_type,
+                                            int bits_per_sample) {
+    if (!f || !plane || !src_frame_ids) return fail(DFTTEST2_B200_EINVAL, "null argument");
+    if (int rc = check_format(sample_type, bits_per_sample)) return rc;
+    if (plane->width <= 0 || plane->height <= 0) return fail(DFTTEST2_B200_EINVAL, "invalid plane size");
+    DeviceGuard dg(f->device);
+    const int bps = bytes_of(sample_type, bits_per_sample);
+    const size_t row = (size_t)plane->width * bps;
+    const size_t frame = row * plane->height;
+    const int T = f->T;
+    const size_t kMaxEntries = f->cache.capacity();
+    SlotGuard sg(f);
+    Slot& s = sg.slot();
+    // device output plane + pinned staging for one upload and the download
+    if (int rc = ensure_bytes(s.d_frames, s.frames_cap, frame, s.done)) return rc;
+    if (int rc = ensure_pinned(s.h_pinned, s.pinned_cap, 2 * frame, s.done)) return rc;
+    CUDA_TRY(cudaEventSynchronize(s.done));
+    uint8_t* h_up = (uint8_t*)s.h_pinned;
+    uint8_t* h_down = h_up + frame;
+
+    int idx[7];
+    int rc = 0;
+    int nacq = 0;
+    for (int t = 0; t < T && rc == 0; ++t) {
+        if (!plane->src[t]) {
+            rc = fail(DFTTEST2_B200_EINVAL, "null source plane");
+            break;
+        }
+        bool upload = false;
+        {
+            std::unique_lock<std::mutex> lk(f->cache_lock);
+            int hit = -1, victim = -1;
+            for (size_t i = 0; i < f->cache.size(); ++i) {
+                auto& e = f->cache[i];
+                if (e.id == src_frame_ids[t] && e.plane == plane_index && e.bytes == frame) {
+                    hit = (int)i;
+                    break;
+                }
+                if (e.refs == 0 && (victim < 0 || e.used < f->cache[victim].used)) victim = (int)i;
+            }
+            if (hit >= 0) {
+                auto& e = f->cache[hit];
+                ++e.refs;
+                e.used = ++f->cache_clock;
+                // another call is queuing this upload: wait until its event is recorded
+                f->cache_cv.wait(lk, [&] { return f->cache[hit].issued; });
+                if (f->cache[hit].id != src_frame_ids[t]) {  // that upload failed
+                    --e.refs;
+                    rc = fail(DFTTEST2_B200_ECUDA, "a concurrent upload of this source plane failed");
+                    break;
+                }
+                idx[t] = hit;
+            } else {
+                if (f->cache.size() < kMaxEntries && (victim < 0 || f->cache.size() < (size_t)(3 * (T + 2)))) {
+                    f->cache.emplace_back();
+                    victim = (int)f->cache.size() - 1;
+                }
+                if (victim < 0) {
+                    rc = fail(DFTTEST2_B200_ENOMEM, "frame cache exhausted (too many concurrent calls)");
+                    break;
+                }
+                auto& e = f->cache[victim];
+                if (!e.ready && cudaEventCreateWithFlags(&e.ready, cudaEventDisableTiming) != cudaSuccess) {
+                    rc = fail(DFTTEST2_B200_ECUDA, "event creation failed");
+                    break;
+                }
+                if (e.cap < frame) {
+                    if (e.d) cudaFree(e.d);
+                    e.d = nullptr;
+                    e.cap = 0;
+                    if (cudaMalloc(&e.d, frame) != cudaSuccess) {
+                        cudaGetLastError();
+                        e.id = -1;
+                        rc = fail(DFTTEST2_B200_ENOMEM, "device allocation failed");
+                        break;
+                    }
+                    e.cap = frame;
+                }
+                e.id = src_frame_ids[t];
+                e.plane = plane_index;
+                e.bytes = frame;
+                e.refs = 1;
+                e.issued = false;
+                e.used = ++f->cache_clock;
+                idx[t] = victim;
+                upload = true;
+            }
+        }
+        ++nacq;
+        auto& e = f->cache[idx[t]];
+        if (upload) {
+            const uint8_t* src = (const uint8_t*)plane->src[t];
+            for (int y = 0; y < plane->height; ++y) std::memcpy(h_up + y * row, src + y * plane->src_stride, row);
+            cudaError_t ce = cudaMemcpyAsync(e.d, h_up, frame, cudaMemcpyHostToDevice, s.stream);
+            if (ce == cudaSuccess) ce = cudaEventRecord(e.ready, s.stream);
+            // the staging buffer is reused by the next upload of this call
+            if (ce == cudaSuccess) ce = cudaEventSynchronize(e.ready);
+            {
+                std::lock_guard<std::mutex> lk(f->cache_lock);
+                if (ce != cudaSuccess) e.id = -1;  // never a hit
+                e.issued = true;
+            }
+            f->cache_cv.notify_all();
+            if (ce != cudaSuccess) rc = fail(DFTTEST2_B200_ECUDA, std::string("upload failed: ") + cudaGetErrorString(ce));
+        } else {
+            if (cudaStreamWaitEvent(s.stream, e.ready, 0) != cudaSuccess) rc = fail(DFTTEST2_B200_ECUDA, "event wait failed");
+        }
+    }
+    if (rc == 0) {
+        dfttest2_b200_plane dp{};
+        for (int t = 0; t < T; ++t) dp.src[t] = f->cache[idx[t]].d;
+        dp.src_stride = row;
+        dp.dst = s.d_frames;
+        dp.dst_stride = row;
+        dp.width = plane->width;
+        dp.height = plane->height;
+        Plan plan;
+        float scale, peak;
+        int kind;
+        scale_peak(sample_type, bits_per_sample, scale, peak, kind);
+        rc = make_plan(f, &dp, 1, bps, plan);
+        if (rc == 0) rc = launch(f, s, plan, kind, scale, peak, s.stream);
+        if (rc == 0) {
+            cudaError_t ce = cudaMemcpyAsync(h_down, s.d_frames, frame, cudaMemcpyDeviceToHost, s.stream);
+            if (ce == cudaSuccess) ce = cudaEventRecord(s.done, s.stream);
+            if (ce == cudaSuccess) ce = cudaEventSynchronize(s.done);
+            if (ce != cudaSuccess) rc = fail(DFTTEST2_B200_ECUDA, std::string("filtering failed: ") + cudaGetErrorString(ce));
+        }
+        if (rc == 0) {
+            uint8_t* dst = (uint8_t*)plane->dst;
+            for (int y = 0; y < plane->height; ++y) std::memcpy(dst + y * plane->dst_stride, h_down + y * row, row);
+        }
+    }
+    {
+        std::lock_guard<std::mutex> lk(f->cache_lock);
+        for (int t = 0; t < nacq; ++t) --f->cache[idx[t]].refs;
+    }
+    return rc;
 }
 
 int dfttest2_b200_process_clip_planes_host(dfttest2_b200_filter* f, const dfttest2_b200_host_plane* hp, int nplanes,

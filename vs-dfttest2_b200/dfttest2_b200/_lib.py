@@ -119,6 +119,7 @@ SIGNATURES = {
         c_int,
         [c_void_p, c_void_p, c_ssize_t, c_ssize_t, c_void_p, c_ssize_t, c_ssize_t, c_int, c_int, c_int, c_int, c_int],
     ),
+    "dfttest2_b200_process_plane_host_cached": (c_int, [c_void_p, POINTER(Plane), POINTER(c_int), c_int, c_int, c_int]),
     "dfttest2_b200_process_clip_planes_host": (c_int, [c_void_p, POINTER(HostPlane), c_int, c_int, c_int, c_int]),
     "dfttest2_b200_process_planes_sigma": (c_int, [c_void_p, POINTER(Plane), c_int, c_int, c_int, c_void_p, c_void_p]),
     "dfttest2_b200_backward_planes": (c_int, [c_void_p, POINTER(GradPlane), c_int, c_void_p, c_void_p, c_void_p]),

@@ -102,6 +102,28 @@ class Filter:
         _lib.check(self._lib.dfttest2_b200_process_plane_host(self.handle, ctypes.byref(pl), sample_type, bits))
         return out
 
+    def process_frame_host_cached(self, frames: np.ndarray, n: int, plane_index: int, sample_type: int,
+                                  bits: int) -> np.ndarray:
+        """Output frame n of one plane of a host clip (N, H, W), as a
+        frame-by-frame host would request it: source planes are cached on the
+        device by (frame number, plane index)."""
+        frames = np.ascontiguousarray(frames)
+        N, h, w = frames.shape
+        r = self.radius
+        ids = [min(max(n - r + t, 0), N - 1) for t in range(2 * r + 1)]
+        out = np.empty((h, w), frames.dtype)
+        pl = _lib.Plane()
+        for t, k in enumerate(ids):
+            pl.src[t] = frames[k].ctypes.data
+        pl.src_stride = frames.strides[1]
+        pl.dst = out.ctypes.data
+        pl.dst_stride = out.strides[0]
+        pl.width, pl.height = w, h
+        arr = (ctypes.c_int * len(ids))(*ids)
+        _lib.check(self._lib.dfttest2_b200_process_plane_host_cached(self.handle, ctypes.byref(pl), arr, plane_index,
+                                                                     sample_type, bits))
+        return out
+
     def process_clip_host(self, frames: np.ndarray, sample_type: int, bits: int) -> np.ndarray:
         """All frames of one plane, (N, H, W) host array."""
         frames = np.ascontiguousarray(frames)
