@@ -68,3 +68,27 @@ def test_cached_concurrent_float(cuda_device):
             assert np.array_equal(got[n], want[n]), n
     finally:
         flt.close()
+
+
+def test_cached_call_rejects_bad_planes(cuda_device):
+    import ctypes
+
+    from dfttest2_b200 import _lib
+
+    flt = Filter(device_id=0, **plugin_arguments(ftype=0, sigma=8.0, tbsize=3))
+    lib = _lib.load()
+    try:
+        src = np.zeros((72, 96), np.uint16)
+        out = np.zeros_like(src)
+        pl = _lib.Plane()
+        for t in range(3):
+            pl.src[t] = src.ctypes.data
+        pl.src_stride, pl.dst, pl.dst_stride, pl.width, pl.height = 192, None, 192, 96, 72
+        ids = (ctypes.c_int * 3)(0, 0, 1)
+        with pytest.raises(_lib.Error, match="null destination"):
+            _lib.check(lib.dfttest2_b200_process_plane_host_cached(flt.handle, ctypes.byref(pl), ids, 0, 0, 16))
+        pl.dst, pl.src_stride = out.ctypes.data, 100
+        with pytest.raises(_lib.Error, match="invalid stride"):
+            _lib.check(lib.dfttest2_b200_process_plane_host_cached(flt.handle, ctypes.byref(pl), ids, 0, 0, 16))
+    finally:
+        flt.close()

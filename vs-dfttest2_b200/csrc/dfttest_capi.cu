@@ -1051,10 +1051,13 @@ int dfttest2_b200_process_plane_host_cached(dfttest2_b200_filter* f, const dftte
     if (!f || !plane || !src_frame_ids) return fail(DFTTEST2_B200_EINVAL, "null argument");
     if (int rc = check_format(sample_type, bits_per_sample)) return rc;
     if (plane->width <= 0 || plane->height <= 0) return fail(DFTTEST2_B200_EINVAL, "invalid plane size");
+    if (!plane->dst) return fail(DFTTEST2_B200_EINVAL, "null destination plane");
     DeviceGuard dg(f->device);
     const int bps = bytes_of(sample_type, bits_per_sample);
     const size_t row = (size_t)plane->width * bps;
     const size_t frame = row * plane->height;
+    if (plane->src_stride < (ptrdiff_t)row || plane->dst_stride < (ptrdiff_t)row)
+        return fail(DFTTEST2_B200_EINVAL, "invalid stride");
     const int T = f->T;
     const size_t kMaxEntries = f->cache.capacity();
     SlotGuard sg(f);
