@@ -125,6 +125,14 @@ int dfttest2_b200_process_plane_host_cached(dfttest2_b200_filter* f, const dftte
                                             const int* src_frame_ids, int plane_index, int sample_type,
                                             int bits_per_sample);
 
+/* The same for several planes of one output frame (the planes of a YUV
+ * frame, one sample format): every plane in one launch and one wait.
+ * plane_indices[i] is the plane index of planes[i]; src_frame_ids as above
+ * (shared by the planes).  nplanes <= 4. */
+int dfttest2_b200_process_frame_host_cached(dfttest2_b200_filter* f, const dfttest2_b200_plane* planes, int nplanes,
+                                            const int* plane_indices, const int* src_frame_ids, int sample_type,
+                                            int bits_per_sample);
+
 /* Whole-clip host path: filters `nframes` frames of one plane stored
  * contiguously in host memory (frame i at src + i*frame_bytes, rows
  * src_stride bytes apart) into dst.  Each source frame is uploaded once

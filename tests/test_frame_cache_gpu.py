@@ -42,6 +42,23 @@ def test_cached_equals_uncached_yuv(order, cuda_device):
         flt.close()
 
 
+def test_frame_call_equals_uncached_planes(cuda_device):
+    """All planes of each frame in one call (one launch) give the per-plane results."""
+    rng = np.random.default_rng(7)
+    planes = [_clip(rng, 7, 96, 160, np.uint8, 255), _clip(rng, 7, 48, 80, np.uint8, 255),
+              _clip(rng, 7, 48, 80, np.uint8, 255)]
+    flt = Filter(device_id=0, **plugin_arguments(ftype=0, sigma=6.0, sbsize=16, sosize=12, tbsize=3))
+    try:
+        for n in (0, 1, 2, 6, 3, 5, 4):
+            got = flt.process_frame_planes_host_cached(planes, n, 0, 8)
+            for p, clip in enumerate(planes):
+                want = _uncached(flt, clip, n, 0, 8)
+                d = np.abs(got[p].astype(np.int64) - want.astype(np.int64))
+                assert d.max() <= 1 and (d == 0).mean() > 0.99, (n, p)
+    finally:
+        flt.close()
+
+
 def test_cached_concurrent_float(cuda_device):
     rng = np.random.default_rng(6)
     clip = _clip(rng, 12, 72, 96, np.float32, 1.0)

@@ -1045,148 +1045,188 @@ int dfttest2_b200_process_plane_host(dfttest2_b200_filter* f, const dfttest2_b20
     return 0;
 }
 
-int dfttest2_b200_process_plane_host_cached(dfttest2_b200_filter* f, const dfttest2_b200_plane* plane,
-                                            const int* src_frame_ids, int plane_index, int sample_type,
+int dfttest2_b200_process_frame_host_cached(dfttest2_b200_filter* f, const dfttest2_b200_plane* planes, int nplanes,
+                                            const int* plane_indices, const int* src_frame_ids, int sample_type,
                                             int bits_per_sample) {
-    if (!f || !plane || !src_frame_ids) return fail(DFTTEST2_B200_EINVAL, "null argument");
+    if (!f || !planes || !plane_indices || !src_frame_ids) return fail(DFTTEST2_B200_EINVAL, "null argument");
+    if (nplanes <= 0 || nplanes > 4) return fail(DFTTEST2_B200_EINVAL, "nplanes must be in [1, 4]");
     if (int rc = check_format(sample_type, bits_per_sample)) return rc;
-    if (plane->width <= 0 || plane->height <= 0) return fail(DFTTEST2_B200_EINVAL, "invalid plane size");
-    if (!plane->dst) return fail(DFTTEST2_B200_EINVAL, "null destination plane");
-    DeviceGuard dg(f->device);
     const int bps = bytes_of(sample_type, bits_per_sample);
-    const size_t row = (size_t)plane->width * bps;
-    const size_t frame = row * plane->height;
-    if (plane->src_stride < (ptrdiff_t)row || plane->dst_stride < (ptrdiff_t)row)
-        return fail(DFTTEST2_B200_EINVAL, "invalid stride");
+    size_t row[4], frame[4], out_off[4], out_total = 0;
+    for (int i = 0; i < nplanes; ++i) {
+        const dfttest2_b200_plane& pl = planes[i];
+        if (pl.width <= 0 || pl.height <= 0) return fail(DFTTEST2_B200_EINVAL, "invalid plane size");
+        if (!pl.dst) return fail(DFTTEST2_B200_EINVAL, "null destination plane");
+        row[i] = (size_t)pl.width * bps;
+        frame[i] = row[i] * pl.height;
+        if (pl.src_stride < (ptrdiff_t)row[i] || pl.dst_stride < (ptrdiff_t)row[i])
+            return fail(DFTTEST2_B200_EINVAL, "invalid stride");
+        for (int t = 0; t < f->T; ++t)
+            if (!pl.src[t]) return fail(DFTTEST2_B200_EINVAL, "null source plane");
+        out_off[i] = out_total;
+        out_total += frame[i];
+    }
+    DeviceGuard dg(f->device);
     const int T = f->T;
     const size_t kMaxEntries = f->cache.capacity();
     SlotGuard sg(f);
     Slot& s = sg.slot();
-    // device output plane + pinned staging for one upload and the download
-    if (int rc = ensure_bytes(s.d_frames, s.frames_cap, frame, s.done)) return rc;
-    if (int rc = ensure_pinned(s.h_pinned, s.pinned_cap, 2 * frame, s.done)) return rc;
+    // device output planes; pinned staging with room for every upload of the call
+    // (so that none waits for another) and for all downloads
+    size_t up_total = 0;
+    for (int i = 0; i < nplanes; ++i) up_total += frame[i] * T;
+    if (int rc = ensure_bytes(s.d_frames, s.frames_cap, out_total, s.done)) return rc;
+    if (int rc = ensure_pinned(s.h_pinned, s.pinned_cap, up_total + out_total, s.done)) return rc;
     CUDA_TRY(cudaEventSynchronize(s.done));
     uint8_t* h_up = (uint8_t*)s.h_pinned;
-    uint8_t* h_down = h_up + frame;
+    uint8_t* h_down = h_up + up_total;
+    size_t up_used = 0;
 
-    int idx[7];
+    int idx[4][7];
+    int acquired[4] = {0, 0, 0, 0};
     int rc = 0;
-    int nacq = 0;
-    for (int t = 0; t < T && rc == 0; ++t) {
-        if (!plane->src[t]) {
-            rc = fail(DFTTEST2_B200_EINVAL, "null source plane");
-            break;
-        }
-        bool upload = false;
-        {
-            std::unique_lock<std::mutex> lk(f->cache_lock);
-            int hit = -1, victim = -1;
-            for (size_t i = 0; i < f->cache.size(); ++i) {
-                auto& e = f->cache[i];
-                if (e.id == src_frame_ids[t] && e.plane == plane_index && e.bytes == frame) {
-                    hit = (int)i;
-                    break;
-                }
-                if (e.refs == 0 && (victim < 0 || e.used < f->cache[victim].used)) victim = (int)i;
-            }
-            if (hit >= 0) {
-                auto& e = f->cache[hit];
-                ++e.refs;
-                e.used = ++f->cache_clock;
-                // another call is queuing this upload: wait until its event is recorded
-                f->cache_cv.wait(lk, [&] { return f->cache[hit].issued; });
-                if (f->cache[hit].id != src_frame_ids[t]) {  // that upload failed
-                    --e.refs;
-                    rc = fail(DFTTEST2_B200_ECUDA, "a concurrent upload of this source plane failed");
-                    break;
-                }
-                idx[t] = hit;
-            } else {
-                if (f->cache.size() < kMaxEntries && (victim < 0 || f->cache.size() < (size_t)(3 * (T + 2)))) {
-                    f->cache.emplace_back();
-                    victim = (int)f->cache.size() - 1;
-                }
-                if (victim < 0) {
-                    rc = fail(DFTTEST2_B200_ENOMEM, "frame cache exhausted (too many concurrent calls)");
-                    break;
-                }
-                auto& e = f->cache[victim];
-                if (!e.ready && cudaEventCreateWithFlags(&e.ready, cudaEventDisableTiming) != cudaSuccess) {
-                    rc = fail(DFTTEST2_B200_ECUDA, "event creation failed");
-                    break;
-                }
-                if (e.cap < frame) {
-                    if (e.d) cudaFree(e.d);
-                    e.d = nullptr;
-                    e.cap = 0;
-                    if (cudaMalloc(&e.d, frame) != cudaSuccess) {
-                        cudaGetLastError();
-                        e.id = -1;
-                        rc = fail(DFTTEST2_B200_ENOMEM, "device allocation failed");
+    for (int i = 0; i < nplanes && rc == 0; ++i) {
+        const dfttest2_b200_plane& pl = planes[i];
+        for (int t = 0; t < T && rc == 0; ++t) {
+            bool upload = false;
+            {
+                std::unique_lock<std::mutex> lk(f->cache_lock);
+                // the cache first grows to a working set for several frames in flight
+                // (4 planes x (2r+1 + 5) frames), then evicts the least recently used
+                // free entry whose buffer already fits (reallocating synchronises the
+                // device), else grows up to its limit, else evicts any free entry
+                int hit = -1, fit = -1, any = -1;
+                for (size_t k = 0; k < f->cache.size(); ++k) {
+                    auto& e = f->cache[k];
+                    if (e.id == src_frame_ids[t] && e.plane == plane_indices[i] && e.bytes == frame[i]) {
+                        hit = (int)k;
                         break;
                     }
-                    e.cap = frame;
+                    if (e.refs != 0) continue;
+                    if (any < 0 || e.used < f->cache[any].used) any = (int)k;
+                    if (e.cap >= frame[i] && (fit < 0 || e.used < f->cache[fit].used)) fit = (int)k;
                 }
-                e.id = src_frame_ids[t];
-                e.plane = plane_index;
-                e.bytes = frame;
-                e.refs = 1;
-                e.issued = false;
-                e.used = ++f->cache_clock;
-                idx[t] = victim;
-                upload = true;
+                const size_t working_set = std::min(kMaxEntries, (size_t)(4 * (T + 5)));
+                int victim = f->cache.size() >= working_set ? fit : -1;
+                if (hit >= 0) {
+                    auto& e = f->cache[hit];
+                    ++e.refs;
+                    e.used = ++f->cache_clock;
+                    // another call is queuing this upload: wait until its event is recorded
+                    f->cache_cv.wait(lk, [&] { return f->cache[hit].issued; });
+                    if (f->cache[hit].id != src_frame_ids[t]) {  // that upload failed
+                        --e.refs;
+                        rc = fail(DFTTEST2_B200_ECUDA, "a concurrent upload of this source plane failed");
+                        break;
+                    }
+                    idx[i][t] = hit;
+                } else {
+                    if (victim < 0 && f->cache.size() < kMaxEntries) {
+                        f->cache.emplace_back();
+                        victim = (int)f->cache.size() - 1;
+                    }
+                    if (victim < 0) victim = any;
+                    if (victim < 0) {
+                        rc = fail(DFTTEST2_B200_ENOMEM, "frame cache exhausted (too many concurrent calls)");
+                        break;
+                    }
+                    auto& e = f->cache[victim];
+                    if (!e.ready && cudaEventCreateWithFlags(&e.ready, cudaEventDisableTiming) != cudaSuccess) {
+                        rc = fail(DFTTEST2_B200_ECUDA, "event creation failed");
+                        break;
+                    }
+                    if (e.cap < frame[i]) {
+                        if (e.d) cudaFree(e.d);
+                        e.d = nullptr;
+                        e.cap = 0;
+                        if (cudaMalloc(&e.d, frame[i]) != cudaSuccess) {
+                            cudaGetLastError();
+                            e.id = -1;
+                            rc = fail(DFTTEST2_B200_ENOMEM, "device allocation failed");
+                            break;
+                        }
+                        e.cap = frame[i];
+                    }
+                    e.id = src_frame_ids[t];
+                    e.plane = plane_indices[i];
+                    e.bytes = frame[i];
+                    e.refs = 1;
+                    e.issued = false;
+                    e.used = ++f->cache_clock;
+                    idx[i][t] = victim;
+                    upload = true;
+                }
             }
-        }
-        ++nacq;
-        auto& e = f->cache[idx[t]];
-        if (upload) {
-            const uint8_t* src = (const uint8_t*)plane->src[t];
-            for (int y = 0; y < plane->height; ++y) std::memcpy(h_up + y * row, src + y * plane->src_stride, row);
-            cudaError_t ce = cudaMemcpyAsync(e.d, h_up, frame, cudaMemcpyHostToDevice, s.stream);
-            if (ce == cudaSuccess) ce = cudaEventRecord(e.ready, s.stream);
-            // the staging buffer is reused by the next upload of this call
-            if (ce == cudaSuccess) ce = cudaEventSynchronize(e.ready);
-            {
-                std::lock_guard<std::mutex> lk(f->cache_lock);
-                if (ce != cudaSuccess) e.id = -1;  // never a hit
-                e.issued = true;
+            ++acquired[i];
+            auto& e = f->cache[idx[i][t]];
+            if (upload) {
+                const uint8_t* src = (const uint8_t*)pl.src[t];
+                uint8_t* stage = h_up + up_used;  // this upload's own staging, in use until the call's final wait
+                up_used += frame[i];
+                for (int y = 0; y < pl.height; ++y) std::memcpy(stage + y * row[i], src + y * pl.src_stride, row[i]);
+                cudaError_t ce = cudaMemcpyAsync(e.d, stage, frame[i], cudaMemcpyHostToDevice, s.stream);
+                if (ce == cudaSuccess) ce = cudaEventRecord(e.ready, s.stream);
+                {
+                    std::lock_guard<std::mutex> lk(f->cache_lock);
+                    if (ce != cudaSuccess) e.id = -1;  // never a hit
+                    e.issued = true;
+                }
+                f->cache_cv.notify_all();
+                if (ce != cudaSuccess) rc = fail(DFTTEST2_B200_ECUDA, std::string("upload failed: ") + cudaGetErrorString(ce));
+            } else {
+                if (cudaStreamWaitEvent(s.stream, e.ready, 0) != cudaSuccess) rc = fail(DFTTEST2_B200_ECUDA, "event wait failed");
             }
-            f->cache_cv.notify_all();
-            if (ce != cudaSuccess) rc = fail(DFTTEST2_B200_ECUDA, std::string("upload failed: ") + cudaGetErrorString(ce));
-        } else {
-            if (cudaStreamWaitEvent(s.stream, e.ready, 0) != cudaSuccess) rc = fail(DFTTEST2_B200_ECUDA, "event wait failed");
         }
     }
     if (rc == 0) {
-        dfttest2_b200_plane dp{};
-        for (int t = 0; t < T; ++t) dp.src[t] = f->cache[idx[t]].d;
-        dp.src_stride = row;
-        dp.dst = s.d_frames;
-        dp.dst_stride = row;
-        dp.width = plane->width;
-        dp.height = plane->height;
+        // every plane of the frame in one launch
+        dfttest2_b200_plane dp[4];
+        for (int i = 0; i < nplanes; ++i) {
+            std::memset(&dp[i], 0, sizeof(dp[i]));
+            for (int t = 0; t < T; ++t) dp[i].src[t] = f->cache[idx[i][t]].d;
+            dp[i].src_stride = row[i];
+            dp[i].dst = (uint8_t*)s.d_frames + out_off[i];
+            dp[i].dst_stride = row[i];
+            dp[i].width = planes[i].width;
+            dp[i].height = planes[i].height;
+        }
         Plan plan;
         float scale, peak;
         int kind;
         scale_peak(sample_type, bits_per_sample, scale, peak, kind);
-        rc = make_plan(f, &dp, 1, bps, plan);
+        rc = make_plan(f, dp, nplanes, bps, plan);
         if (rc == 0) rc = launch(f, s, plan, kind, scale, peak, s.stream);
         if (rc == 0) {
-            cudaError_t ce = cudaMemcpyAsync(h_down, s.d_frames, frame, cudaMemcpyDeviceToHost, s.stream);
+            cudaError_t ce = cudaMemcpyAsync(h_down, s.d_frames, out_total, cudaMemcpyDeviceToHost, s.stream);
             if (ce == cudaSuccess) ce = cudaEventRecord(s.done, s.stream);
             if (ce == cudaSuccess) ce = cudaEventSynchronize(s.done);
             if (ce != cudaSuccess) rc = fail(DFTTEST2_B200_ECUDA, std::string("filtering failed: ") + cudaGetErrorString(ce));
         }
         if (rc == 0) {
-            uint8_t* dst = (uint8_t*)plane->dst;
-            for (int y = 0; y < plane->height; ++y) std::memcpy(dst + y * plane->dst_stride, h_down + y * row, row);
+            for (int i = 0; i < nplanes; ++i) {
+                uint8_t* dst = (uint8_t*)planes[i].dst;
+                const uint8_t* src = h_down + out_off[i];
+                for (int y = 0; y < planes[i].height; ++y)
+                    std::memcpy(dst + y * planes[i].dst_stride, src + y * row[i], row[i]);
+            }
         }
     }
+    // uploads queued by this call read its staging: on failure, let them finish first
+    if (rc != 0) cudaStreamSynchronize(s.stream);
     {
         std::lock_guard<std::mutex> lk(f->cache_lock);
-        for (int t = 0; t < nacq; ++t) --f->cache[idx[t]].refs;
+        for (int i = 0; i < nplanes; ++i)
+            for (int t = 0; t < acquired[i]; ++t) --f->cache[idx[i][t]].refs;
     }
     return rc;
+}
+
+int dfttest2_b200_process_plane_host_cached(dfttest2_b200_filter* f, const dfttest2_b200_plane* plane,
+                                            const int* src_frame_ids, int plane_index, int sample_type,
+                                            int bits_per_sample) {
+    if (!plane) return fail(DFTTEST2_B200_EINVAL, "null argument");
+    return dfttest2_b200_process_frame_host_cached(f, plane, 1, &plane_index, src_frame_ids, sample_type,
+                                                   bits_per_sample);
 }
 
 int dfttest2_b200_process_clip_planes_host(dfttest2_b200_filter* f, const dfttest2_b200_host_plane* hp, int nplanes,

@@ -120,6 +120,8 @@ SIGNATURES = {
         [c_void_p, c_void_p, c_ssize_t, c_ssize_t, c_void_p, c_ssize_t, c_ssize_t, c_int, c_int, c_int, c_int, c_int],
     ),
     "dfttest2_b200_process_plane_host_cached": (c_int, [c_void_p, POINTER(Plane), POINTER(c_int), c_int, c_int, c_int]),
+    "dfttest2_b200_process_frame_host_cached": (
+        c_int, [c_void_p, POINTER(Plane), c_int, POINTER(c_int), POINTER(c_int), c_int, c_int]),
     "dfttest2_b200_process_clip_planes_host": (c_int, [c_void_p, POINTER(HostPlane), c_int, c_int, c_int, c_int]),
     "dfttest2_b200_process_planes_sigma": (c_int, [c_void_p, POINTER(Plane), c_int, c_int, c_int, c_void_p, c_void_p]),
     "dfttest2_b200_backward_planes": (c_int, [c_void_p, POINTER(GradPlane), c_int, c_void_p, c_void_p, c_void_p]),

@@ -124,6 +124,31 @@ class Filter:
                                                                      sample_type, bits))
         return out
 
+    def process_frame_planes_host_cached(self, clips: Sequence[np.ndarray], n: int, sample_type: int,
+                                         bits: int) -> list:
+        """Output frame n of every plane of a host clip (one (N, H_i, W_i)
+        array per plane), in one call: the frame-by-frame path with the device
+        frame cache, all planes in one launch."""
+        clips = [np.ascontiguousarray(c) for c in clips]
+        N = clips[0].shape[0]
+        r = self.radius
+        ids = [min(max(n - r + t, 0), N - 1) for t in range(2 * r + 1)]
+        arr = (_lib.Plane * len(clips))()
+        outs = []
+        for pl, c in zip(arr, clips):
+            _, h, w = c.shape
+            o = np.empty((h, w), c.dtype)
+            for t, k in enumerate(ids):
+                pl.src[t] = c[k].ctypes.data
+            pl.src_stride, pl.dst, pl.dst_stride = c.strides[1], o.ctypes.data, o.strides[0]
+            pl.width, pl.height = w, h
+            outs.append(o)
+        pidx = (ctypes.c_int * len(clips))(*range(len(clips)))
+        fids = (ctypes.c_int * len(ids))(*ids)
+        _lib.check(self._lib.dfttest2_b200_process_frame_host_cached(self.handle, arr, len(clips), pidx, fids,
+                                                                     sample_type, bits))
+        return outs
+
     def process_clip_host(self, frames: np.ndarray, sample_type: int, bits: int) -> np.ndarray:
         """All frames of one plane, (N, H, W) host array."""
         frames = np.ascontiguousarray(frames)
