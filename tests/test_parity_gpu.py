@@ -1,6 +1,6 @@
 """Parity of the CUDA path (through the C ABI) with the reference.
 
-Bars (from the task's north star):
+Bars:
 * float32 planes: max-abs error <= 2e-5 of full scale (1.0);
 * 8/16-bit planes: within 1 LSB, exact-match fraction reported (and
   required to stay high).
