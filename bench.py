@@ -280,7 +280,7 @@ def run_batch(opts):
     device = torch.device("cuda", 0)
     torch.cuda.set_device(device)
     lib = _lib.load()
-    specs = synth.batch_specs(opts.seed)
+    specs = synth.batch_specs(opts.seed, small=opts.workload == "batch_small")
     items, calls, pairs = [], [], []
     total_frames = 0
     flops = 0.0
@@ -354,7 +354,9 @@ def run_batch(opts):
         "unit": "frames/s", "n_gpus": 1, "steps": opts.steps, "warmup": opts.warmup, "ms_per_step": bat_ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded sinusoids + gaussian 0.03, built on the device)",
-        "config": {"workload": f"32 clips (synth.batch_specs seed {opts.seed}): 640x360..3840x2160, 4..32 frames, "
+        "config": {"workload": f"32 clips (synth.batch_specs seed {opts.seed}"
+                               f"{', small' if opts.workload == 'batch_small' else ''}): "
+                               f"{'640x360' if opts.workload == 'batch_small' else '640x360..3840x2160'}, 4..32 frames, "
                                "GRAYS/YUV420P8/YUV420P16, sbsize 8/16/32 sosize 3/4, tbsize 1/3/5, ftype 0/1",
                    "frames": total_frames, "l2": "inputs of several GB > L2, no flush"},
         "sequential_ms": seq_ms, "batch_ms": bat_ms, "speedup": seq_ms / bat_ms, "tune_seconds": tune_s,
@@ -377,15 +379,16 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-peak", action="store_true", help="skip the SGEMM peak measurement (profiling runs)")
-    ap.add_argument("--workload", default="yuv1080p", choices=["yuv1080p", "batch"],
-                    help="batch: the 32-clip multi-clip batching workload (one GPU)")
+    ap.add_argument("--workload", default="yuv1080p", choices=["yuv1080p", "batch", "batch_small"],
+                    help="batch: the 32-clip multi-clip batching workload (one GPU); batch_small: the same with "
+                         "640x360 clips only")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--fbf-frames", type=int, default=32,
                     help="frames filtered frame by frame through the cached per-plane host path (0 skips)")
     ap.add_argument("--tc-steps", type=int, default=10,
                     help="steps timed for each tensor-core precision mode (0 skips the comparison)")
     opts = ap.parse_args()
-    if opts.workload == "batch":
+    if opts.workload in ("batch", "batch_small"):
         if opts.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no multi-clip batch"}))
             return

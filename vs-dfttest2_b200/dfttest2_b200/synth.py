@@ -97,15 +97,16 @@ def make_clip_device(fmt: VideoFormat, width: int, height: int, frames: int, see
     return planes
 
 
-def batch_specs(seed: int = 0, nclips: int = 32) -> list[dict]:
+def batch_specs(seed: int = 0, nclips: int = 32, small: bool = False) -> list[dict]:
     """Clips of the multi-clip batching workload: resolution from {640x360,
-    1280x720, 1920x1080, 3840x2160}, 4..32 frames, GRAYS / YUV420P8 /
-    YUV420P16, sbsize in {8, 16, 32} with sosize = 3/4 sbsize, tbsize in
-    {1, 3, 5}, ftype in {0, 1}, flat sigma ~ U[2, 16]."""
+    1280x720, 1920x1080, 3840x2160} (only 640x360 with `small`, a case
+    where single clips leave the GPU partly idle), 4..32 frames, GRAYS /
+    YUV420P8 / YUV420P16, sbsize in {8, 16, 32} with sosize = 3/4 sbsize,
+    tbsize in {1, 3, 5}, ftype in {0, 1}, flat sigma ~ U[2, 16]."""
     from .clip import GRAYS, YUV420P8, YUV420P16
 
     rng = np.random.default_rng(seed)
-    res = [(640, 360), (1280, 720), (1920, 1080), (3840, 2160)]
+    res = [(640, 360)] * 4 if small else [(640, 360), (1280, 720), (1920, 1080), (3840, 2160)]
     fmts = [GRAYS, YUV420P8, YUV420P16]
     out = []
     for i in range(nclips):
