@@ -822,10 +822,29 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
                 const int py = by * S + r;
                 float2* cell = reinterpret_cast<float2*>(s_ola + (py % B) * pitch + px);
                 float2 acc = *cell;
-                for (int k = b_lo; k <= b_hi; ++k) {
-                    const float2 v = *reinterpret_cast<const float2*>(s_wbuf + k * L::BSTR + TL::off(r, px - k * S));
-                    acc.x += v.x;
-                    acc.y += v.y;
+                if (B == 4 * S) {
+                    // at most four blocks: their loads are issued together, then
+                    // summed in ascending block order
+                    float2 v[4];
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) {
+                        const int k = b_hi - 3 + m;
+                        v[m] = k >= b_lo ? *reinterpret_cast<const float2*>(s_wbuf + k * L::BSTR + TL::off(r, px - k * S))
+                                         : make_float2(0.f, 0.f);
+                    }
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) {
+                        if (b_hi - 3 + m >= b_lo) {
+                            acc.x += v[m].x;
+                            acc.y += v[m].y;
+                        }
+                    }
+                } else {
+                    for (int k = b_lo; k <= b_hi; ++k) {
+                        const float2 v = *reinterpret_cast<const float2*>(s_wbuf + k * L::BSTR + TL::off(r, px - k * S));
+                        acc.x += v.x;
+                        acc.y += v.y;
+                    }
                 }
                 if (r < nfin) {
                     finish(py, px, acc.x);
