@@ -646,6 +646,7 @@ __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefe
 // ---------------------------------------------------------------------------
 template <int B, int T, int NW, int FC, int MINB = 1>
 __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __grid_constant__ KernelArgs a) {
+    static_assert((B & (B - 1)) == 0, "ring rows are indexed with a mask of B - 1");
     using L = Layout<B, T, NW>;
     using TL = Tile<B>;
     constexpr int M = B / 2;
@@ -735,7 +736,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
         const int r = div_small(rem, inv_rl);
         const int lx = rem - r * rowlen;
         const int py = r_lo + r;
-        soff = (t * B + (py % B)) * pitch + lx;
+        soff = (t * B + (py & (B - 1))) * pitch + lx;
         gidx = (long long)mirror(py - oy, Hh) * job.src_stride + mirror(x0 + lx - ox, W);
     };
     const float inv_rl = 1.0f / (float)rowlen;
@@ -766,7 +767,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
         // ---- per-warp block transforms (B lanes per block, BPW blocks per warp)
         {
             // row phase: the DC of each block is summed over its rows with shuffles
-            const float dc = row_task<B, T>(wbl, s_in, pitch, (by * S + lw) % B, blr * S, s_win, lw, vec, valid);
+            const float dc = row_task<B, T>(wbl, s_in, pitch, (by * S + lw) & (B - 1), blr * S, s_win, lw, vec, valid);
             const float tot = block_row_sum<B>(dc);
             // g = DC / Re(WF[0]) (cpu_source/kernel.hpp:1945)
             if (lw == 0 && valid) s_g[bl] = P.g_div != 0.0f ? __fdiv_rn(tot, P.g_div) : 0.0f;
@@ -820,17 +821,23 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
                 const int b_lo = px <= B - 2 ? 0 : div_small(px - B + 1 + S, inv_S);
                 const int b_hi = min(div_small(px, inv_S), nbx - 1);
                 const int py = by * S + r;
-                float2* cell = reinterpret_cast<float2*>(s_ola + (py % B) * pitch + px);
+                float2* cell = reinterpret_cast<float2*>(s_ola + (py & (B - 1)) * pitch + px);
                 float2 acc = *cell;
                 if (B == 4 * S) {
                     // at most four blocks: their loads are issued together, then
-                    // summed in ascending block order
+                    // summed in ascending block order. Block k = b_hi - 3 + m
+                    // holds the pair at x = x_top + (3 - m) S, x_top = px - b_hi S;
+                    // S is a multiple of 4, so only the 4-float chunk index moves
+                    const int x_top = px - b_hi * S;
+                    const int off0 = (b_hi - 3) * L::BSTR + r * B + (x_top & 3);
+                    const int c0 = x_top >> 2, sw = TL::swz(r), sq = S >> 2;
                     float2 v[4];
 #pragma unroll
                     for (int m = 0; m < 4; ++m) {
-                        const int k = b_hi - 3 + m;
-                        v[m] = k >= b_lo ? *reinterpret_cast<const float2*>(s_wbuf + k * L::BSTR + TL::off(r, px - k * S))
-                                         : make_float2(0.f, 0.f);
+                        v[m] = b_hi - 3 + m >= b_lo
+                                   ? *reinterpret_cast<const float2*>(s_wbuf + off0 + m * L::BSTR +
+                                                                      (((c0 + (3 - m) * sq) ^ sw) << 2))
+                                   : make_float2(0.f, 0.f);
                     }
 #pragma unroll
                     for (int m = 0; m < 4; ++m) {
@@ -860,7 +867,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
                 const int b_lo = px <= B - 1 ? 0 : div_small(px - B + S, inv_S);
                 const int b_hi = min(div_small(px, inv_S), nbx - 1);
                 const int py = by * S + r;
-                float* cell = s_ola + (py % B) * pitch + px;
+                float* cell = s_ola + (py & (B - 1)) * pitch + px;
                 float acc = *cell;
                 for (int k = b_lo; k <= b_hi; ++k) acc += s_wbuf[k * L::BSTR + TL::off(r, px - k * S)];
                 if (r < nfin) {
