@@ -554,7 +554,10 @@ def main():
                 ids = [min(max(n - r + t, 0), N - 1) for t in range(2 * r + 1)]
                 for t, k in enumerate(ids):
                     pl.src[t] = src[k].ctypes.data
-                out = np.empty((ph, pw), src.dtype)
+                # touched once, as the pooled frames of a frame server are (a first write
+                # into fresh pages would time page faults, not the library)
+                out = np.zeros((ph, pw), src.dtype)
+                out.fill(1)
                 pl.src_stride = pw * 2
                 pl.dst = out.ctypes.data
                 pl.dst_stride = pw * 2
