@@ -12,6 +12,7 @@ import numpy as np
 import pytest
 
 from conftest import golden_planes, load_case, load_plane
+from dfttest2_b200 import _lib
 from dfttest2_b200.frontend import plugin_arguments
 from dfttest2_b200.plugin import Filter
 from oracle import oracle as O
@@ -94,7 +95,8 @@ def test_against_reference_build(cfg, cuda_device):
 
 
 @pytest.mark.parametrize("B,sosize,tb", [(8, 6, 1), (8, 6, 3), (8, 4, 5), (16, 12, 3), (32, 24, 1), (32, 16, 3),
-                                         (16, 8, 1), (32, 24, 5)])
+                                         (16, 8, 1), (32, 24, 5), (32, 24, 7), (32, 24, 3), (32, 28, 3),
+                                         (16, 12, 5), (16, 12, 7), (16, 0, 5), (32, 0, 3), (16, 0, 7)])
 @pytest.mark.parametrize("dtype,bits", [(np.float32, 32), (np.uint16, 16)])
 def test_against_fp64_oracle(B, sosize, tb, dtype, bits, cuda_device):
     rng = np.random.default_rng(B + tb)
@@ -106,6 +108,17 @@ def test_against_fp64_oracle(B, sosize, tb, dtype, bits, cuda_device):
     out = gpu_plane(frames, args, bits)
     exact = check(out, ref, bits, f"B{B} S{B - sosize} T{tb}")
     print(f"B{B} T{tb} {dtype.__name__}: exact-match vs FP64 {exact:.4f}")
+
+
+def test_unsplittable_plane_is_rejected(cuda_device):
+    """sosize 31 of 32 needs strips of at least 31 blocks, wider than the
+    kernel's strips: the call fails with a clear message instead of leaving
+    strips unfiltered."""
+    rng = np.random.default_rng(5)
+    frames = _frames(rng, 3, 91, 109, np.float32, 32)
+    args = plugin_arguments(ftype=0, sigma=5.0, sbsize=32, sosize=31, tbsize=3)
+    with pytest.raises(_lib.Error, match="no split"):
+        gpu_plane(frames, args, 32)
 
 
 def test_device_path_equals_host_path(cuda_device):

@@ -97,7 +97,9 @@ int prepare_group(dfttest2_b200_batch* b, dfttest2_b200_batch::Group& g, int var
     const Variant& var = g.cands[var_idx];
     g.var_idx = var_idx;
     g.target_mult = target_mult;
-    plan_units(g.B, g.S, var.nw * var.bpw, g.planes, (long long)target_mult * b->num_sms, g.plan);
+    if (int rc = plan_units(g.B, g.S, strip_blocks(var, g.B, g.S), g.planes, (long long)target_mult * b->num_sms,
+                            g.plan))
+        return rc;
     const size_t smem = var.smem(g.plan.pitch);
     if (smem > 227 * 1024) return fail(DFTTEST2_B200_EINVAL, "block step too large for the kernel's shared memory");
     KernelFn kern = g.generic ? var.generic : var.main;
@@ -154,7 +156,10 @@ int tune_group(dfttest2_b200_batch* b, dfttest2_b200_batch::Group& g, cudaStream
     int rc = 0;
     for (int v = 0; v < (int)g.cands.size() && rc == 0; ++v) {
         for (int t : kTargets) {
-            if ((rc = prepare_group(b, g, v, t)) != 0) break;
+            if ((rc = prepare_group(b, g, v, t)) != 0) {
+                if (v > 0 && rc == DFTTEST2_B200_EINVAL) rc = 0;  // an alternative shape that cannot split these planes
+                break;
+            }
             if (v == last_v && g.plan.nunits == last_units) continue;  // same split as the previous target
             last_v = v;
             last_units = g.plan.nunits;
@@ -248,7 +253,7 @@ int dfttest2_b200_batch_create(const dfttest2_b200_clip* clips, int nclips, int 
             g->S = f->S;
             g->T = f->T;
             g->generic = generic;
-            g->cands = candidate_variants(f->B, f->T);
+            g->cands = candidate_variants(f->B, f->T, f->S);
             if (g->cands.empty()) return fail(DFTTEST2_B200_EINVAL, "unsupported block_size / radius");
         }
         const int r = f->radius;

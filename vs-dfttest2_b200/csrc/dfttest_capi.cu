@@ -79,10 +79,15 @@ Variant make_variant() {
 
 // kernel variants per (block size, temporal size): NW warps per CTA keeps
 // the per-warp block buffers plus the rings within 227 KB of shared memory
-// (and 16 warps cap registers at 128 per thread). 16x16x3 runs two 10-warp
+// (and 16 warps cap registers at 128 per thread). Strips must be at least
+// (B-S)/S blocks wide, so a shape needs enough blocks per step to split
+// every plane width: 32x32 shapes have at least 5 (sosize 24 needs 5 for
+// some widths; larger overlaps need more, and planes that cannot be split
+// are rejected). 32x32 blocks with 3 to 7 frames keep their tables in
+// global memory, which leaves room for those strips. 16x16x3 runs two 10-warp
 // CTAs per SM (96 registers per thread): 20 warps hide more latency than
 // two 8-warp CTAs at 128 registers (2.5 % faster on the 1080p workload).
-Variant select_variant(int B, int T) {
+Variant select_variant(int B, int T, int S) {
     // DFTTEST2_B200_WARPS=16 / 8 / 4 select other 16x16x3 shapes
     const char* env = std::getenv("DFTTEST2_B200_WARPS");
     if (env && B == 16 && T == 3 && std::atoi(env) == 16) return make_variant<16, 3, 16>();
@@ -111,9 +116,10 @@ Variant select_variant(int B, int T) {
     case 32:
         switch (T) {
         case 1: return make_variant<32, 1, 16>();
-        case 3: return make_variant<32, 3, 8>();
-        case 5: return make_variant<32, 5, 4>();
-        case 7: return make_variant<32, 7, 2>();
+        // two 6-warp CTAs per SM unless the overlap needs wider strips (sosize 26 and up)
+        case 3: return S >= 7 ? make_variant<32, 3, 6, 2>() : make_variant<32, 3, 8>();
+        case 5: return make_variant<32, 5, 5>();
+        case 7: return make_variant<32, 7, 5>();
         }
         break;
 #endif
@@ -121,18 +127,31 @@ Variant select_variant(int B, int T) {
     return Variant{};
 }
 
+// Blocks per strip for a kernel shape and block step: the shape's blocks per
+// step, fewer when the rings for a large step would not fit in the 227 KB of
+// shared memory a CTA may have.
+int strip_blocks(const Variant& v, int B, int S) {
+    constexpr size_t kMaxSmem = 227 * 1024;
+    int w = v.nw * v.bpw;
+    while (w > 1 && v.smem((((w * S) + (B - S)) + 3) & ~3) > kMaxSmem) --w;
+    return w;
+}
+
 // Kernel shapes the batch autotuner may time besides select_variant's
 // choice: other warp counts per CTA for the block sizes and temporal sizes of
 // multi-clip batches (fewer warps per CTA = narrower strips, more CTAs).
-std::vector<Variant> candidate_variants(int B, int T) {
+std::vector<Variant> candidate_variants(int B, int T, int S) {
     std::vector<Variant> v;
-    v.push_back(select_variant(B, T));
+    v.push_back(select_variant(B, T, S));
     if (!v.back().main) return {};
 #ifndef DFTTEST2_B200_ONLY_B16
     if (B == 8 && T == 1) v.push_back(make_variant<8, 1, 8, 2>());
     if (B == 8 && T == 3) v.push_back(make_variant<8, 3, 8, 2>());
     if (B == 32 && T == 1) v.push_back(make_variant<32, 1, 8>());
-    if (B == 32 && T == 3) v.push_back(make_variant<32, 3, 4, 2>());
+    if (B == 32 && T == 3) {
+        v.push_back(S >= 7 ? make_variant<32, 3, 8>() : make_variant<32, 3, 6, 2>());
+        v.push_back(make_variant<32, 3, 4, 2>());
+    }
 #endif
     if (B == 16 && T == 1) v.push_back(make_variant<16, 1, 8, 2>());
     if (B == 16 && T == 3) {
@@ -330,7 +349,11 @@ struct PlaneRef {
 // BPS blocks per step: strips of at most BPS blocks; each strip is cut into
 // segments until the launch has about `target` units (segments no shorter
 // than max(O/S, 4) blocks).
-void plan_units(int B, int S, int BPS, const std::vector<PlaneRef>& planes, long long target, Plan& plan) {
+// Fails (EINVAL) when some plane has no strip split whose strips are at
+// least O/S blocks wide (so that the two edge bands of a strip stay apart)
+// and at most BPS blocks wide (the kernel's blocks per step); the unit
+// kernel would otherwise skip the wider strips.
+int plan_units(int B, int S, int BPS, const std::vector<PlaneRef>& planes, long long target, Plan& plan) {
     const int O = B - S;
     const int n = (int)planes.size();
     plan.jobs.resize(n);
@@ -363,6 +386,12 @@ void plan_units(int B, int S, int BPS, const std::vector<PlaneRef>& planes, long
         j.nsy = std::max(1, std::min(nsy, pny / min_seg));
         // strips must be at least O/S blocks wide so that bands do not overlap
         while (j.nsx > 1 && pnx / j.nsx < (O + S - 1) / S) --j.nsx;
+        if ((pnx + j.nsx - 1) / j.nsx > BPS)
+            return fail(DFTTEST2_B200_EINVAL,
+                        "sbsize " + std::to_string(B) + " / sosize " + std::to_string(O) + " on a plane " +
+                            std::to_string(p.width) + " wide: no split into strips of " +
+                            std::to_string((O + S - 1) / S) + " to " + std::to_string(BPS) +
+                            " blocks (use a smaller sosize)");
         j.unit_base = unit;
         j.fix_base = fix;
         j.seam_base = seams;
@@ -379,6 +408,7 @@ void plan_units(int B, int S, int BPS, const std::vector<PlaneRef>& planes, long
     plan.pitch = ((BPS * S + O) + 3) & ~3;
     plan.nseams = seams;
     plan.full_strips = full;
+    return 0;
 }
 
 // the mirror padding must stay inside the plane (cpu_source/getframe_impl.cpp:44-62 reads 2*ox - x)
@@ -430,13 +460,12 @@ int make_plan(const dfttest2_b200_filter* f, const dfttest2_b200_plane* planes, 
     // units go out in plan order: tall planes first (their strips are the
     // longest units), so that short units fill the last wave
     std::stable_sort(refs.begin(), refs.end(), [](const PlaneRef& x, const PlaneRef& y) { return x.height > y.height; });
-    const int BPS = f->var.nw * f->var.bpw;
+    const int BPS = strip_blocks(f->var, f->B, f->S);
     const int nsy = choose_nsy(refs, f->B, f->S, BPS, std::max(1, f->var.minb) * f->num_sms);
     long long strips_total = 0;
     for (const PlaneRef& r : refs) strips_total += (dft2::pad_num(r.width, f->B, f->S) + BPS - 1) / BPS;
     // plan_units derives nsy = ceil(target / strips) = nsy from this target
-    plan_units(f->B, f->S, BPS, refs, nsy > 1 ? nsy * strips_total : 1, plan);
-    return 0;
+    return plan_units(f->B, f->S, BPS, refs, nsy > 1 ? nsy * strips_total : 1, plan);
 }
 
 // ---- tensor-core form ------------------------------------------------------
@@ -854,7 +883,7 @@ int dfttest2_b200_create(const dfttest2_b200_params* p, dfttest2_b200_filter** o
     f->pmin = (float)p->pmin;
     f->pmax = (float)p->pmax;
     f->syn_slice = syn;
-    f->var = select_variant(B, T);
+    f->var = select_variant(B, T, f->S);
     if (!f->var.main) return fail(DFTTEST2_B200_EINVAL, "unsupported block_size / radius");
 
     // -- tables --------------------------------------------------------------
@@ -1603,7 +1632,7 @@ extern "C" int dfttest2_b200_process_plane_noalloc(const dfttest2_b200_params* p
     const int syn = p->synthesis_slice < 0 ? radius : p->synthesis_slice;
     if (syn >= T) return fail(DFTTEST2_B200_EINVAL, "\"synthesis_slice\" out of range");
     if (int rc = check_format(sample_type, bits_per_sample)) return rc;
-    const Variant var = select_variant(B, T);
+    const Variant var = select_variant(B, T, S);
     if (!var.main) return fail(DFTTEST2_B200_EINVAL, "unsupported block_size / radius");
 
     // -- tables (same layout as dfttest2_b200_create builds) -----------------
@@ -1685,9 +1714,13 @@ extern "C" int dfttest2_b200_process_plane_noalloc(const dfttest2_b200_params* p
     if (dev != device_id) return fail(DFTTEST2_B200_EINVAL, "invalid device_id");
     CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
 
-    const int BPS = var.nw * var.bpw;
+    const int BPS = strip_blocks(var, B, S);
     const int pnx = dft2::pad_num(plane->width, B, S), pny = dft2::pad_num(plane->height, B, S);
-    const int nsx = (pnx + BPS - 1) / BPS;
+    // strips of at least O/S blocks (their edge bands stay apart) and at most BPS
+    int nsx = (pnx + BPS - 1) / BPS;
+    while (nsx > 1 && pnx / nsx < (O + S - 1) / S) --nsx;
+    if ((pnx + nsx - 1) / nsx > BPS)
+        return fail(DFTTEST2_B200_EINVAL, "sosize too large for this sbsize and plane width (no valid strip split)");
     const int min_seg = std::max((O + S - 1) / S, 4);
     const size_t off_err = 0, off_job = 256;
     const size_t off_win = align256(off_job + sizeof(dft2::PlaneJob));

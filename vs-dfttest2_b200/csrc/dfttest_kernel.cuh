@@ -263,23 +263,33 @@ template <int B> struct Tile {
     __device__ static __forceinline__ int off(int y, int x) { return y * B + ((((x >> 2) ^ swz(y)) << 2) | (x & 3)); }
 };
 
+// Large blocks (32x32 with 3, 5 or 7 frames) read the window,
+// synthesis-window and gain tables from global memory (L1-cached) and run the
+// row phase in two passes, which leaves shared memory and registers for wide
+// enough strips and more warps; smaller blocks keep the tables in shared
+// memory (faster for them: 16x16x5 with global tables ran 17 % slower).
+template <int B, int T> struct Large {
+    static constexpr bool value = B == 32 && T >= 3;
+};
+
 template <int B, int T, int NW>
 struct Layout {
     static constexpr int M = B / 2;
     static constexpr int BPW = 32 / B;
     static constexpr int WP = B + 4;
     static constexpr int NSLOT = M + 2;
+    static constexpr int TAB = Large<B, T>::value ? 0 : 1;  // tables held in shared memory
     // warp-buffer floats per block; the stride is 4 (mod 32) floats so that the
     // overlap-add, whose lanes read the same 16-byte chunk of consecutive
     // blocks, spreads over 8 bank groups
     static constexpr int BSTR = T * B * B + 4;
     // offsets in floats (ring sizes depend on the runtime pitch)
     static constexpr int o_win = 0;
-    static constexpr int o_wsyn = o_win + T * B * WP;
-    static constexpr int o_sig = o_wsyn + B * WP;
-    static constexpr int o_sig2 = o_sig + T * NSLOT * B;
-    static constexpr int o_wfe = o_sig2 + T * NSLOT * B;
-    static constexpr int o_g = o_wfe + 2 * T * NSLOT * B;
+    static constexpr int o_wsyn = o_win + TAB * T * B * WP;
+    static constexpr int o_sig = o_wsyn + TAB * B * WP;
+    static constexpr int o_sig2 = o_sig + TAB * T * NSLOT * B;
+    static constexpr int o_wfe = o_sig2 + TAB * T * NSLOT * B;
+    static constexpr int o_g = o_wfe + TAB * 2 * T * NSLOT * B;
     static constexpr int o_wbuf = o_g + ((NW * BPW + 3) & ~3);
     static constexpr int o_ring = o_wbuf + NW * BPW * BSTR;
     __host__ __device__ static int in_ring_floats(int pitch) { return T * B * pitch; }
@@ -288,6 +298,15 @@ struct Layout {
         return sizeof(float) * (size_t)(o_ring + in_ring_floats(pitch) + ola_floats(pitch));
     }
 };
+
+// a table element: shared memory, or global memory through the read-only path
+template <bool G> __device__ __forceinline__ float ldt(const float* p) { return G ? __ldg(p) : *p; }
+template <bool G> __device__ __forceinline__ float2 ldt2(const float* p) {
+    return G ? __ldg(reinterpret_cast<const float2*>(p)) : *reinterpret_cast<const float2*>(p);
+}
+template <bool G> __device__ __forceinline__ float4 ldt4(const float* p) {
+    return G ? __ldg(reinterpret_cast<const float4*>(p)) : *reinterpret_cast<const float4*>(p);
+}
 
 // i / n for small non-negative i, n through a float reciprocal (exact while
 // i * n < 2^22, which the shared-memory extents guarantee)
@@ -299,25 +318,33 @@ __device__ __forceinline__ int div_small(int i, float inv_n) { return __float2in
 // ---------------------------------------------------------------------------
 template <int B, int T>
 __device__ __forceinline__ float row_task(float* __restrict__ wb, const float* __restrict__ ring, int pitch, int slot_y,
-                                          int xoff, const float* __restrict__ win, int y, bool vec, bool store) {
+                                          int xoff, const float* __restrict__ win, float wscale, int y, bool vec,
+                                          bool store) {
     using TL = Tile<B>;
     constexpr int H = B / 2;
     constexpr int R = (T - 1) / 2;
-    float X[T][B];
+    constexpr bool G = Large<B, T>::value;
+    constexpr int WPITCH = G ? B : TL::WP;
     // frames in centre-first order (t' = 0 is frame r): the temporal DFT of the
     // shifted sequence is w^(p r) times that of the original, which is the
-    // centre-frame weight of the inverse, so the inverse becomes a plain sum
-#pragma unroll
-    for (int t = 0; t < T; ++t) {
+    // centre-frame weight of the inverse, so the inverse becomes a plain sum.
+    // Windowed row of frame t'; a global window table is scaled here, giving
+    // the same product scale * window (rounded once) as the shared table.
+    auto windowed_row = [&](int t, float (&v)[B]) {
         const int ft = (t + R) % T;
         const float* src = ring + (ft * B + slot_y) * pitch + xoff;
-        const float* w = win + (ft * B + y) * TL::WP;
-        float v[B];
+        const float* w = win + (ft * B + y) * WPITCH;
         if (vec) {
 #pragma unroll
             for (int q = 0; q < B / 4; ++q) {
                 const float4 s4 = *reinterpret_cast<const float4*>(src + 4 * q);
-                const float4 w4 = *reinterpret_cast<const float4*>(w + 4 * q);
+                float4 w4 = ldt4<G>(w + 4 * q);
+                if (G) {
+                    w4.x *= wscale;
+                    w4.y *= wscale;
+                    w4.z *= wscale;
+                    w4.w *= wscale;
+                }
                 v[4 * q + 0] = s4.x * w4.x;
                 v[4 * q + 1] = s4.y * w4.y;
                 v[4 * q + 2] = s4.z * w4.z;
@@ -325,66 +352,155 @@ __device__ __forceinline__ float row_task(float* __restrict__ wb, const float* _
             }
         } else {
 #pragma unroll
-            for (int x = 0; x < B; ++x) v[x] = src[x] * w[x];
+            for (int x = 0; x < B; ++x) v[x] = src[x] * (G ? wscale * __ldg(w + x) : w[x]);
         }
-        if constexpr (B == 8) r2c_8(v, X[t]);
-        if constexpr (B == 16) r2c_16(v, X[t]);
-        if constexpr (B == 32) r2c_32(v, X[t]);
-    }
-    // temporal DFT over the T frames (plane p = temporal bin)
-    if constexpr (T > 1) {
-        // x-bins 0 and B/2: two real sequences
-        float a_re[R + 1], a_im[R + 1], b_re[R + 1], b_im[R + 1];
-        {
-            float xa[T], xb[T];
+    };
+    auto r2c = [](float (&v)[B], float (&X)[B]) {
+        if constexpr (B == 8) r2c_8(v, X);
+        if constexpr (B == 16) r2c_16(v, X);
+        if constexpr (B == 32) r2c_32(v, X);
+    };
+    if constexpr (G && T > 1) {
+        // Two passes: every frame's row spectrum goes to its plane of the block
+        // buffer (registers for T x B spectra would leave room for few warps),
+        // then the temporal DFT runs in place, one 4-float chunk (two packed
+        // x-bins) at a time. The lane owns row y of every plane of its block
+        // buffer, so no barrier is needed; lanes of a block past the strip end
+        // work on their own (unused) buffer.
 #pragma unroll
-            for (int t = 0; t < T; ++t) {
-                xa[t] = X[t][0];
-                xb[t] = X[t][1];
-            }
-            if constexpr (T == 3) { rdftT_3(xa, a_re, a_im); rdftT_3(xb, b_re, b_im); }
-            if constexpr (T == 5) { rdftT_5(xa, a_re, a_im); rdftT_5(xb, b_re, b_im); }
-            if constexpr (T == 7) { rdftT_7(xa, a_re, a_im); rdftT_7(xb, b_re, b_im); }
+        for (int t = 0; t < T; ++t) {
+            float v[B], X[B];
+            windowed_row(t, v);
+            r2c(v, X);
+            float* dst = wb + t * B * B;
+#pragma unroll
+            for (int q = 0; q < B / 4; ++q)
+                *reinterpret_cast<float4*>(dst + TL::off(y, 4 * q)) =
+                    make_float4(X[4 * q], X[4 * q + 1], X[4 * q + 2], X[4 * q + 3]);
         }
-        X[0][0] = a_re[0];
-        X[0][1] = b_re[0];
-#pragma unroll
-        for (int p = 1; p <= R; ++p) {
-            X[p][0] = a_re[p];
-            X[p][1] = a_im[p];
-            X[T - p][0] = b_re[p];
-            X[T - p][1] = b_im[p];
-        }
-#pragma unroll
-        for (int c = 1; c < H; ++c) {
-            float re[T], im[T];
-#pragma unroll
-            for (int t = 0; t < T; ++t) {
-                re[t] = X[t][2 * c];
-                im[t] = X[t][2 * c + 1];
-            }
+        auto cdft = [](float (&re)[T], float (&im)[T]) {
             if constexpr (T == 3) cdft_3_fwd(re, im);
             if constexpr (T == 5) cdft_5_fwd(re, im);
             if constexpr (T == 7) cdft_7_fwd(re, im);
+        };
+        float dc = 0.0f;
+#pragma unroll
+        for (int q = 0; q < B / 4; ++q) {
+            float4 z[T];
+#pragma unroll
+            for (int t = 0; t < T; ++t) z[t] = *reinterpret_cast<const float4*>(wb + t * B * B + TL::off(y, 4 * q));
+            float re[T], im[T];
+            if (q == 0) {
+                // x-bins 0 and B/2: two real sequences
+                float xa[T], xb[T], a_re[R + 1], a_im[R + 1], b_re[R + 1], b_im[R + 1];
+#pragma unroll
+                for (int t = 0; t < T; ++t) {
+                    xa[t] = z[t].x;
+                    xb[t] = z[t].y;
+                }
+                if constexpr (T == 3) { rdftT_3(xa, a_re, a_im); rdftT_3(xb, b_re, b_im); }
+                if constexpr (T == 5) { rdftT_5(xa, a_re, a_im); rdftT_5(xb, b_re, b_im); }
+                if constexpr (T == 7) { rdftT_7(xa, a_re, a_im); rdftT_7(xb, b_re, b_im); }
+                z[0].x = a_re[0];
+                z[0].y = b_re[0];
+#pragma unroll
+                for (int p = 1; p <= R; ++p) {
+                    z[p].x = a_re[p];
+                    z[p].y = a_im[p];
+                    z[T - p].x = b_re[p];
+                    z[T - p].y = b_im[p];
+                }
+                dc = a_re[0];
+            } else {
+#pragma unroll
+                for (int t = 0; t < T; ++t) {
+                    re[t] = z[t].x;
+                    im[t] = z[t].y;
+                }
+                cdft(re, im);
+#pragma unroll
+                for (int t = 0; t < T; ++t) {
+                    z[t].x = re[t];
+                    z[t].y = im[t];
+                }
+            }
 #pragma unroll
             for (int t = 0; t < T; ++t) {
-                X[t][2 * c] = re[t];
-                X[t][2 * c + 1] = im[t];
+                re[t] = z[t].z;
+                im[t] = z[t].w;
+            }
+            cdft(re, im);
+#pragma unroll
+            for (int t = 0; t < T; ++t) {
+                z[t].z = re[t];
+                z[t].w = im[t];
+                *reinterpret_cast<float4*>(wb + t * B * B + TL::off(y, 4 * q)) = z[t];
             }
         }
-    }
-    if (store) {
+        return dc;
+    } else {
+        float X[T][B];
 #pragma unroll
-        for (int p = 0; p < T; ++p) {
-            float* dst = wb + p * B * B;
+        for (int t = 0; t < T; ++t) {
+            float v[B];
+            windowed_row(t, v);
+            r2c(v, X[t]);
+        }
+        // temporal DFT over the T frames (plane p = temporal bin)
+        if constexpr (T > 1) {
+            // x-bins 0 and B/2: two real sequences
+            float a_re[R + 1], a_im[R + 1], b_re[R + 1], b_im[R + 1];
+            {
+                float xa[T], xb[T];
 #pragma unroll
-            for (int q = 0; q < B / 4; ++q) {
-                *reinterpret_cast<float4*>(dst + TL::off(y, 4 * q)) =
-                    make_float4(X[p][4 * q], X[p][4 * q + 1], X[p][4 * q + 2], X[p][4 * q + 3]);
+                for (int t = 0; t < T; ++t) {
+                    xa[t] = X[t][0];
+                    xb[t] = X[t][1];
+                }
+                if constexpr (T == 3) { rdftT_3(xa, a_re, a_im); rdftT_3(xb, b_re, b_im); }
+                if constexpr (T == 5) { rdftT_5(xa, a_re, a_im); rdftT_5(xb, b_re, b_im); }
+                if constexpr (T == 7) { rdftT_7(xa, a_re, a_im); rdftT_7(xb, b_re, b_im); }
+            }
+            X[0][0] = a_re[0];
+            X[0][1] = b_re[0];
+#pragma unroll
+            for (int p = 1; p <= R; ++p) {
+                X[p][0] = a_re[p];
+                X[p][1] = a_im[p];
+                X[T - p][0] = b_re[p];
+                X[T - p][1] = b_im[p];
+            }
+#pragma unroll
+            for (int c = 1; c < H; ++c) {
+                float re[T], im[T];
+#pragma unroll
+                for (int t = 0; t < T; ++t) {
+                    re[t] = X[t][2 * c];
+                    im[t] = X[t][2 * c + 1];
+                }
+                if constexpr (T == 3) cdft_3_fwd(re, im);
+                if constexpr (T == 5) cdft_5_fwd(re, im);
+                if constexpr (T == 7) cdft_7_fwd(re, im);
+#pragma unroll
+                for (int t = 0; t < T; ++t) {
+                    X[t][2 * c] = re[t];
+                    X[t][2 * c + 1] = im[t];
+                }
             }
         }
+        if (store) {
+#pragma unroll
+            for (int p = 0; p < T; ++p) {
+                float* dst = wb + p * B * B;
+#pragma unroll
+                for (int q = 0; q < B / 4; ++q) {
+                    *reinterpret_cast<float4*>(dst + TL::off(y, 4 * q)) =
+                        make_float4(X[p][4 * q], X[p][4 * q + 1], X[p][4 * q + 2], X[p][4 * q + 3]);
+                }
+            }
+        }
+        return X[0][0];
     }
-    return X[0][0];
 }
 
 // sum over the B lanes of one block; lanes of a block are contiguous
@@ -409,27 +525,27 @@ template <int M> __device__ __forceinline__ void half_dft_inv(float (&re)[M], fl
 }
 
 // gain of the M bins a lane holds; slot tables are [NSLOT][B] per plane
-template <int M, int B, int FC, bool ZM>
+template <int M, int B, int FC, bool ZM, bool G>
 __device__ __forceinline__ void gain_lane_zm(float (&re)[M], float (&im)[M], const float* __restrict__ sig,
                                              const float* __restrict__ sig2, const float* __restrict__ wfe, int w,
                                              float g, bool dual, const FilterParams& a) {
 #pragma unroll
     for (int j = 0; j < M; ++j) {
-        const float s = sig[j * B + w];
-        const float s2 = (FC != kFilterWiener && dual) ? sig2[j * B + w] : s;
-        const float2 wv = ZM ? reinterpret_cast<const float2*>(wfe)[j * B + w] : make_float2(0.0f, 0.0f);
+        const float s = ldt<G>(sig + j * B + w);
+        const float s2 = (FC != kFilterWiener && dual) ? ldt<G>(sig2 + j * B + w) : s;
+        const float2 wv = ZM ? ldt2<G>(wfe + 2 * (j * B + w)) : make_float2(0.0f, 0.0f);
         apply_bin<FC, ZM>(re[j], im[j], s, s2, dual, wv, g, a);
     }
 }
 
-template <int M, int B, int FC>
+template <int M, int B, int FC, bool G>
 __device__ __forceinline__ void gain_lane(float (&re)[M], float (&im)[M], const float* __restrict__ sig,
                                           const float* __restrict__ sig2, const float* __restrict__ wfe, int w, float g,
                                           bool dual, bool has_w, const FilterParams& a) {
     if (has_w)
-        gain_lane_zm<M, B, FC, true>(re, im, sig, sig2, wfe, w, g, dual, a);
+        gain_lane_zm<M, B, FC, true, G>(re, im, sig, sig2, wfe, w, g, dual, a);
     else
-        gain_lane_zm<M, B, FC, false>(re, im, sig, sig2, wfe, w, g, dual, a);
+        gain_lane_zm<M, B, FC, false, G>(re, im, sig, sig2, wfe, w, g, dual, a);
 }
 
 // x *= (c + i s) for a compile-time constant (after unrolling) twiddle
@@ -483,6 +599,7 @@ __device__ __forceinline__ void column_task(float* __restrict__ wb, float g, con
     constexpr int M = B / 2;
     constexpr int R = (T - 1) / 2;
     constexpr int NS = M + 2;
+    constexpr bool G = Large<B, T>::value;  // tables in global memory
     const int c = w >> 1, h = w & 1;
     const bool packed = (c == 0);
     const bool dual = dual_tables && packed;
@@ -511,8 +628,8 @@ __device__ __forceinline__ void column_task(float* __restrict__ wb, float g, con
 #pragma unroll
     for (int p = 1; p < T; ++p) {
         load_half(wb + p * B * B);
-        gain_lane<M, B, FC>(qr, qi, sm_sig + p * NS * B, sm_sig2 + p * NS * B, sm_wfe + 2 * p * NS * B, w, g, dual,
-                            (a.wmask >> p) & 1, a);
+        gain_lane<M, B, FC, G>(qr, qi, sm_sig + p * NS * B, sm_sig2 + p * NS * B, sm_wfe + 2 * p * NS * B, w, g, dual,
+                               (a.wmask >> p) & 1, a);
         // the centre-frame weight w^(p r) is already in the spectrum (centre-first
         // frame order); the packed lane enters a B-column plane multiplied by i
         if (packed && p > R) {
@@ -567,13 +684,15 @@ __device__ __forceinline__ void column_task(float* __restrict__ wb, float g, con
             qi[M / 2] = 0.0f;
         }
     }
-    gain_lane<M, B, FC>(qr, qi, sm_sig, sm_sig2, sm_wfe, w, g, dual, a.wmask & 1, a);
+    gain_lane<M, B, FC, G>(qr, qi, sm_sig, sm_sig2, sm_wfe, w, g, dual, a.wmask & 1, a);
     if (packed) {
         if (h == 0) {
-            const float2 w1 = reinterpret_cast<const float2*>(sm_wfe)[M * B + w];
-            const float2 w2 = reinterpret_cast<const float2*>(sm_wfe)[(M + 1) * B + w];
-            apply_bin<FC>(e1r, e1i, sm_sig[M * B + w], dual ? sm_sig2[M * B + w] : 0.0f, dual, w1, g, a);
-            apply_bin<FC>(e2r, e2i, sm_sig[(M + 1) * B + w], dual ? sm_sig2[(M + 1) * B + w] : 0.0f, dual, w2, g, a);
+            const float2 w1 = ldt2<G>(sm_wfe + 2 * (M * B + w));
+            const float2 w2 = ldt2<G>(sm_wfe + 2 * ((M + 1) * B + w));
+            apply_bin<FC>(e1r, e1i, ldt<G>(sm_sig + M * B + w), dual ? ldt<G>(sm_sig2 + M * B + w) : 0.0f, dual, w1,
+                          g, a);
+            apply_bin<FC>(e2r, e2i, ldt<G>(sm_sig + (M + 1) * B + w), dual ? ldt<G>(sm_sig2 + (M + 1) * B + w) : 0.0f,
+                          dual, w2, g, a);
             sr[0] += qr[0];
             si[0] += e1r;
             sr[M / 2] += qr[M / 2];
@@ -615,9 +734,10 @@ __device__ __forceinline__ void column_task(float* __restrict__ wb, float g, con
 }
 
 // inverse rows: packed row -> real, synthesis window, in place
-template <int B>
+template <int B, bool G>
 __device__ __forceinline__ void inverse_row_task(float* __restrict__ wb, const float* __restrict__ wsyn, int y) {
     using TL = Tile<B>;
+    constexpr int WPITCH = G ? B : TL::WP;
     float v[B], o[B];
 #pragma unroll
     for (int q = 0; q < B / 4; ++q) {
@@ -630,10 +750,10 @@ __device__ __forceinline__ void inverse_row_task(float* __restrict__ wb, const f
     if constexpr (B == 8) c2r_8(v, o);
     if constexpr (B == 16) c2r_16(v, o);
     if constexpr (B == 32) c2r_32(v, o);
-    const float* w = wsyn + y * TL::WP;
+    const float* w = wsyn + y * WPITCH;
 #pragma unroll
     for (int q = 0; q < B / 4; ++q) {
-        const float4 w4 = *reinterpret_cast<const float4*>(w + 4 * q);
+        const float4 w4 = ldt4<G>(w + 4 * q);
         *reinterpret_cast<float4*>(wb + TL::off(y, 4 * q)) =
             make_float4(o[4 * q] * w4.x, o[4 * q + 1] * w4.y, o[4 * q + 2] * w4.z, o[4 * q + 3] * w4.w);
     }
@@ -700,6 +820,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
     const float inv_scale = 1.0f / P.scale;  // exact for the power-of-two integer scales
 
     // --- constants into shared memory -----------------------------------
+    constexpr bool G = Large<B, T>::value;  // tables read from global memory
     float* s_win = sm + L::o_win;
     float* s_wsyn = sm + L::o_wsyn;
     float* s_sig = sm + L::o_sig;
@@ -710,14 +831,21 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
     float* s_in = sm + L::o_ring;
     float* s_ola = s_in + L::in_ring_floats(pitch);
     // scale * window, rounded once as in load_block (cpu_source/getframe_impl.cpp:137)
-    for (int i = tid; i < T * B * B; i += NT) s_win[(i / B) * TL::WP + (i % B)] = P.scale * P.win[i];
-    for (int i = tid; i < B * B; i += NT) s_wsyn[(i / B) * TL::WP + (i % B)] = P.wsyn[i];
     const bool dual_tables = (FC != kFilterWiener) && P.sig2 != nullptr;
-    for (int i = tid; i < T * L::NSLOT * B; i += NT) {
-        s_sig[i] = P.sig[i];
-        if (dual_tables) s_sig2[i] = P.sig2[i];
+    if constexpr (!G) {
+        for (int i = tid; i < T * B * B; i += NT) s_win[(i / B) * TL::WP + (i % B)] = P.scale * P.win[i];
+        for (int i = tid; i < B * B; i += NT) s_wsyn[(i / B) * TL::WP + (i % B)] = P.wsyn[i];
+        for (int i = tid; i < T * L::NSLOT * B; i += NT) {
+            s_sig[i] = P.sig[i];
+            if (dual_tables) s_sig2[i] = P.sig2[i];
+        }
+        for (int i = tid; i < 2 * T * L::NSLOT * B; i += NT) s_wfe[i] = P.wfe[i];
     }
-    for (int i = tid; i < 2 * T * L::NSLOT * B; i += NT) s_wfe[i] = P.wfe[i];
+    const float* t_win = G ? P.win : s_win;
+    const float* t_wsyn = G ? P.wsyn : s_wsyn;
+    const float* t_sig = G ? P.sig : s_sig;
+    const float* t_sig2 = G ? P.sig2 : s_sig2;
+    const float* t_wfe = G ? P.wfe : s_wfe;
     for (int i = tid; i < L::ola_floats(pitch); i += NT) s_ola[i] = 0.0f;
 
     const int fw = u.fw;
@@ -767,14 +895,15 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
         // ---- per-warp block transforms (B lanes per block, BPW blocks per warp)
         {
             // row phase: the DC of each block is summed over its rows with shuffles
-            const float dc = row_task<B, T>(wbl, s_in, pitch, (by * S + lw) & (B - 1), blr * S, s_win, lw, vec, valid);
+            const float dc =
+                row_task<B, T>(wbl, s_in, pitch, (by * S + lw) & (B - 1), blr * S, t_win, P.scale, lw, vec, valid);
             const float tot = block_row_sum<B>(dc);
             // g = DC / Re(WF[0]) (cpu_source/kernel.hpp:1945)
             if (lw == 0 && valid) s_g[bl] = P.g_div != 0.0f ? __fdiv_rn(tot, P.g_div) : 0.0f;
             __syncwarp();
-            column_task<B, T, FC>(wbl, s_g[bl], s_sig, s_sig2, s_wfe, lw, dual_tables, valid, P);
+            column_task<B, T, FC>(wbl, s_g[bl], t_sig, t_sig2, t_wfe, lw, dual_tables, valid, P);
             __syncwarp();
-            if (valid) inverse_row_task<B>(wbl, s_wsyn, lw);
+            if (valid) inverse_row_task<B, G>(wbl, t_wsyn, lw);
         }
         __syncthreads();  // block outputs complete; this step's input rows consumed
 
