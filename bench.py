@@ -44,7 +44,7 @@ SLOCATION = [0.0, 12.0, 1 / 3, 28 / 3, 2 / 3, 20 / 3, 1.0, 4.0]
 FLOP_PER_BLOCK = {1: 9473, 3: 26385, 5: 47329, 7: 74033}  # B = 16, reference codelet counts
 METRIC = "1080p YUV420P16 frames/s (DFTTest sbsize16 sosize12 tbsize3, all planes)"
 # DRAM bytes (read + write) of the unit kernel per 1080p YUV420P16 frame, from one ncu capture of a
-# 24-frame launch (profiles/dfttest_unit_16x3_yuv420p16.md); traffic grows with the frames processed
+# 24-frame launch of this workload; traffic grows with the frames processed
 DRAM_BYTES_PER_FRAME = 18_990_699
 
 
@@ -213,6 +213,7 @@ def cpu_reference_fps(args, planes, seconds_target=15.0, threads=None):
     threads = threads or os.cpu_count() or 1
     kind = "reference" if O.ref_available() else "port"
     full = dict(args)
+    isa = O.ref_isa() if kind == "reference" else "scalar C (FP64 port)"
 
     def one(n):
         for p in range(3):
@@ -233,7 +234,8 @@ def cpu_reference_fps(args, planes, seconds_target=15.0, threads=None):
     with ThreadPoolExecutor(threads) as ex:
         list(ex.map(one, [i % nf for i in range(sample)]))
     dt = time.perf_counter() - t0
-    return {"value": sample / dt, "unit": "frames/s", "cores": threads, "kind": kind,
+    return {"value": sample / dt, "unit": "frames/s", "cores": threads, "kind": kind, "isa": isa,
+            "cpu_model": O.cpu_model(),
             "sample": f"{sample} output frames (3 planes each) of the 1080p YUV420P16 workload, "
                       f"frames in parallel over {threads} threads"}
 
@@ -243,8 +245,8 @@ def run_reference(opts, rank, world):
         return
     args = workload_args()
     planes = make_planes(0, 8, args["radius"])
-    for _ in range(opts.warmup):
-        pass
+    for _ in range(opts.warmup):  # pages, caches and thread pool warmed on a short sample
+        cpu_reference_fps(args, planes, seconds_target=1.0)
     vals = []
     base = None
     for _ in range(opts.steps):
@@ -262,6 +264,11 @@ def run_reference(opts, rank, world):
 
 
 def run_batch(opts):
+    """Prints the multi-clip batching workload's line (batch_measure)."""
+    print(json.dumps(batch_measure(opts.seed, opts.workload == "batch_small", opts.steps, opts.warmup)))
+
+
+def batch_measure(seed, small, steps, warmup):
     """Multi-clip batching workload: 32 seeded clips of mixed resolution,
     length, format and block parameters (synth.batch_specs), filtered by one
     graph launch of a tuned batch vs 32 sequential plain calls (one
@@ -271,6 +278,9 @@ def run_batch(opts):
     import ctypes
 
     import torch
+
+    from types import SimpleNamespace
+    opts = SimpleNamespace(seed=seed, workload="batch_small" if small else "batch", steps=steps, warmup=warmup)
 
     from dfttest2_b200 import _lib, frontend as fe, synth
     from dfttest2_b200.autograd import frame_planes
@@ -366,7 +376,94 @@ def run_batch(opts):
         "clocks": clocks.summary(),
     }
     batch.close()
-    print(json.dumps(result))
+    for flt, *_ in calls:
+        flt.close()
+    return result
+
+
+def autograd_measure(steps=10, warmup=3):
+    """Differentiation workload: 8 GRAYS float32 clips of 256x256 x 9 frames
+    (seeded sinusoids; noisy = clean + Gaussian noise, sigma ~ U[0.02, 0.08]
+    per clip), Wiener, sbsize 16 / sosize 12 / tbsize 3, learnable sigma array
+    (3, 16, 9) initialised to 0.05, MSE to the clean clips.  Times the forward
+    pass alone and forward + backward (adjoint kernel) with CUDA events."""
+    import torch
+
+    from dfttest2_b200 import GRAYS
+    from dfttest2_b200.autograd import DFTTestModule
+    from dfttest2_b200.frontend import plugin_arguments
+    from dfttest2_b200.synth import make_clip
+
+    device = torch.device("cuda", 0)
+    rng = np.random.default_rng(4)
+    noisy, clean = [], []
+    for c in range(8):
+        _, cl = make_clip(GRAYS, 256, 256, 9, seed=400 + c, noise_sigma=0.0)
+        x = cl.planes[0]
+        clean.append(x)
+        noisy.append(x + rng.standard_normal(x.shape).astype(np.float32) * np.float32(rng.uniform(0.02, 0.08)))
+    x = torch.from_numpy(np.stack(noisy)).to(device)
+    target = torch.from_numpy(np.stack(clean)).to(device)
+    mod = DFTTestModule(plugin_arguments(ftype=0, sbsize=16, sosize=12, tbsize=3), 0.05, device="cuda:0")
+    stream = torch.cuda.current_stream(device)
+
+    def fwd():
+        with torch.no_grad():
+            return mod(x)
+
+    def fwd_bwd():
+        xg = x.detach().requires_grad_(True)
+        loss = (mod(xg) - target).pow(2).mean()
+        loss.backward()
+        return loss
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    f_ms = timed(fwd)
+    fb_ms = timed(fwd_bwd)
+    mod.flt.close()
+    return {"fwd_ms": f_ms, "fwd_bwd_ms": fb_ms, "ratio": fb_ms / f_ms, "steps": steps,
+            "workload": "8 GRAYS float32 clips 256x256 x 9 frames, sbsize16 sosize12 tbsize3, learnable sigma "
+                        "(3,16,9) = 0.05, MSE to clean; forward vs forward + backward (adjoint kernel)"}
+
+
+def reference_parity(args, host_planes, outs, frames, r):
+    """Max LSB and exact-match fraction of device outputs against the
+    reference's CPU math (oracle/_ref) on sampled output frames, all planes.
+    `outs` are (N, H, W) int16 CUDA tensors indexed like host_planes' output
+    frames (output frame n reads host frames n-r..n+r)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import oracle as O
+
+    if not O.ref_available():
+        return None
+    jobs = [(p, n) for p in range(3) for n in frames]
+
+    def one(job):
+        p, n = job
+        return O.ref_plane(O.clip_frames(host_planes[p], n, r), args, 16)
+
+    with ThreadPoolExecutor(min(len(jobs), os.cpu_count() or 1)) as ex:
+        refs = list(ex.map(one, jobs))
+    worst, exact, total = 0, 0, 0
+    for (p, n), ref in zip(jobs, refs):
+        got = outs[p][n].cpu().numpy().view(np.uint16)
+        d = np.abs(got.astype(np.int64) - ref.astype(np.int64))
+        worst = max(worst, int(d.max()))
+        exact += int((d == 0).sum())
+        total += d.size
+    return {"max_lsb": worst, "exact": exact / total, "frames": list(frames), "checker": "oracle/_ref (reference CPU math)"}
 
 
 def main():
@@ -387,6 +484,10 @@ def main():
                     help="frames filtered frame by frame through the cached per-plane host path (0 skips)")
     ap.add_argument("--tc-steps", type=int, default=10,
                     help="steps timed for each tensor-core precision mode (0 skips the comparison)")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "tc_bf16x3", "tc_tf32", "tc_bf16"],
+                    help="arithmetic of the timed steps (profiling runs of the tensor-core form)")
+    ap.add_argument("--extras", type=int, default=1,
+                    help="0 skips the parity, differentiation and batching keys (profiling runs)")
     opts = ap.parse_args()
     if opts.workload in ("batch", "batch_small"):
         if opts.impl == "reference":
@@ -444,6 +545,9 @@ def main():
     def step():
         flt.process_planes_device(planes, 0, 16, stream.cuda_stream)
 
+    if opts.precision != "fp32":
+        flt.set_precision(opts.precision)
+
     clocks = ClockSampler(local).__enter__()  # started early: nvidia-smi takes a moment to produce samples
     for _ in range(opts.warmup):
         step()
@@ -469,16 +573,26 @@ def main():
     frames_done = world * (hi - lo) * opts.steps
     value = frames_done / (ms * 1e-3)
     ms_per_step = ms / opts.steps
+    flt.check()  # raises if a kernel reported a failure during the timed steps
+    extras = opts.extras and world == 1 and opts.precision == "fp32"
+    # parity of the timed outputs against the reference's CPU math on two sampled frames
+    sample_frames = (0, (hi - lo) // 2 + 1)
+    parity = {}
+    if extras:
+        parity["fp32"] = reference_parity(args, host_planes, dev_out, sample_frames, r)
 
     # ---- tensor-core form of the transforms on the same workload, against the plain FP32 output
     tc_results = {}
-    if opts.tc_steps > 0:
+    if opts.tc_steps > 0 and opts.precision == "fp32":
         plain_out = [o.clone() for o in dev_out]
         for mode in ("tc_bf16x3", "tc_tf32"):
             flt.set_precision(mode)
             for _ in range(2):
                 step()
             torch.cuda.synchronize()
+            flt.check()
+            if extras and mode == "tc_bf16x3":
+                parity[mode] = reference_parity(args, host_planes, dev_out, sample_frames, r)
             t_start, t_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             t_start.record(stream)
             for _ in range(opts.tc_steps):
@@ -619,8 +733,8 @@ def main():
         "gpu_launches": launches_per_step * opts.steps,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": DRAM_BYTES_PER_FRAME * (hi - lo),
-                     "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum per launch, scaled from a 24-frame "
-                                     "ncu capture (profiles/dfttest_unit_16x3_yuv420p16.md)",
+                     "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum per launch, scaled from an ncu "
+                                     "capture of a 24-frame launch",
                      "peak_source": "cuBLAS FP32 SGEMM (TF32 off) measured in this run; nominal 148 SM x 128 x 2 x "
                                     "1.965 GHz = 74.4",
                      "flop_per_step": flops_step, "hbm_algorithmic_gbs": algo_bytes / (ms_per_step * 1e-3) / 1e9,
@@ -628,8 +742,15 @@ def main():
                      "hbm_peak_source": measured_peaks().get("source")},
         "clocks": clocks.summary(),
         "tc": tc_results,
+        "parity": parity or None,
         "e2e_frame_by_frame": fbf or None,
     }
+    if extras:
+        result["fwd_bwd_over_fwd"] = autograd_measure()
+        bm = batch_measure(0, True, 5, 2)
+        result["batch_speedup"] = {"value": bm["speedup"], "sequential_ms": bm["sequential_ms"],
+                                   "batch_ms": bm["batch_ms"], "gpu_launches": bm["gpu_launches"],
+                                   "parity": bm["parity"], "workload": bm["config"]["workload"]}
     if world == 1 and rank == 0 and not opts.no_cpu_baseline:
         result["cpu_baseline"] = cpu_reference_fps(args, host_planes)
     flt.close()

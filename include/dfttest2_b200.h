@@ -105,6 +105,27 @@ void dfttest2_b200_free(dfttest2_b200_filter* f);
 int dfttest2_b200_process_planes(dfttest2_b200_filter* f, const dfttest2_b200_plane* planes, int nplanes,
                                  int sample_type, int bits_per_sample, void* stream);
 
+/* Kernel status of the asynchronous calls (process_planes,
+ * process_planes_sigma, the tensor-core form).  The kernels record an
+ * internal failure (a unit wider than the kernel's strip, a bounded wait for
+ * the tensor cores that ran out) in an error word of the stream slot instead
+ * of trapping; this waits for the filter's queued work, clears the words and
+ * returns DFTTEST2_B200_EKERNEL with the failure's text if any was set.  The
+ * host-memory calls below (process_plane_host, the cached and clip paths)
+ * read the word after their own wait and return DFTTEST2_B200_EKERNEL
+ * themselves.  The reference reports every CUDA failure through
+ * setFilterError (cuda_source/source.cpp:124-138, 418-421). */
+int dfttest2_b200_check(dfttest2_b200_filter* f);
+
+/* Iteration limit of the filter's bounded device waits (the tensor-core
+ * form's waits for its products); a negative value restores the default
+ * (2^22 polls).  A limit of 0 makes every such wait give up at once: the
+ * kernel then drains the products in flight with the default limit, frees
+ * its tensor memory, returns early and the call reports
+ * DFTTEST2_B200_EKERNEL.  Meant for failure-path tests; no counterpart in
+ * the reference. */
+int dfttest2_b200_set_wait_limit(dfttest2_b200_filter* f, int iterations);
+
 /* Host-memory path with the semantics of DFTTestGetFrame for one plane:
  * copies the 2r+1 source planes in, filters, copies the result out and
  * waits for completion.  Concurrent calls are spread over num_streams
@@ -286,6 +307,12 @@ void dfttest2_b200_batch_free(dfttest2_b200_batch* b);
  * concurrent host threads) race: serialise them on one stream. */
 int dfttest2_b200_process_plane_noalloc(const dfttest2_b200_params* params, const dfttest2_b200_plane* plane,
                                         int sample_type, int bits_per_sample, void* stream);
+
+/* Kernel status of the last dfttest2_b200_process_plane_noalloc call on
+ * device_id: waits for `stream`, then reads the error word in the same static
+ * array (allocates nothing) and returns DFTTEST2_B200_EKERNEL with the
+ * failure's text if the kernels reported one.  No reference counterpart. */
+int dfttest2_b200_noalloc_check(int device_id, void* stream);
 
 /* RDFT: FP64 direct real DFT over 1, 2 or 3 axes, real last axis first
  * (cpu_source/source.cpp:269-340).  `out` receives

@@ -25,7 +25,40 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 FP64_LIB = os.path.join(HERE, "liboracle.so")
-REF_LIB = os.path.join(HERE, "_ref", "libdfttest_ref.so")
+REF_LIB_V3 = os.path.join(HERE, "_ref", "libdfttest_ref.so")      # x86-64-v3 (AVX2)
+REF_LIB_V4 = os.path.join(HERE, "_ref", "libdfttest_ref_v4.so")   # x86-64-v4 (AVX-512)
+
+
+def _cpu_flags() -> set:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    return set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return set()
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def ref_isa() -> str:
+    """ISA of the reference build this host runs: the AVX-512 build where the
+    CPU has the x86-64-v4 extensions (as dfttest2_cpu's dispatch picks its
+    widest build, cpu_source/source.cpp:221-265), else the AVX2 build."""
+    v4 = {"avx512f", "avx512bw", "avx512dq", "avx512vl"}
+    return "x86-64-v4" if v4 <= _cpu_flags() and os.path.exists(REF_LIB_V4) else "x86-64-v3"
+
+
 
 _fp64 = None
 _ref = None
@@ -53,15 +86,15 @@ def _load_fp64():
 
 
 def ref_available() -> bool:
-    return os.path.exists(REF_LIB)
+    return os.path.exists(REF_LIB_V3)
 
 
 def _load_ref():
     global _ref
     if _ref is None:
         if not ref_available():
-            raise FileNotFoundError(f"{REF_LIB} not built (needs the reference tree; see oracle/Makefile)")
-        lib = ctypes.CDLL(REF_LIB)
+            raise FileNotFoundError(f"{REF_LIB_V3} not built (needs the reference tree; see oracle/Makefile)")
+        lib = ctypes.CDLL(REF_LIB_V4 if ref_isa() == "x86-64-v4" else REF_LIB_V3)
         lib.ref_dfttest_plane.restype = c_int
         lib.ref_dfttest_plane.argtypes = [
             POINTER(c_void_p), c_int, c_int, c_int, c_int, c_int, c_void_p, c_int, POINTER(c_double),

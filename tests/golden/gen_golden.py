@@ -1,7 +1,8 @@
 #!/usr/bin/env python3
 """Generates the golden fixtures in tests/golden/ from the reference itself.
 
-Runs only where the reference tree is present (read-only, at REF below).
+Runs only where the reference tree is present (read-only); its path comes from
+the DFTTEST2_REF environment variable.
 
 * Plugin arguments: the reference's own Python front end
   (python/dfttest2.py DFTTest -> DFTTest2, python/helpers.py) is imported
@@ -29,7 +30,8 @@ import types
 
 import numpy as np
 
-REF = "/root/reference"
+# the reference tree (vs-dfttest2 sources), given by the caller; no default
+REF = os.environ.get("DFTTEST2_REF", "")
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path[:0] = [ROOT, os.path.join(ROOT, "vs-dfttest2_b200")]
@@ -124,6 +126,9 @@ def synthetic(seed, n, h, w, dtype, bits):
 
 def main():
     from oracle import oracle as O
+
+    if not REF or not os.path.isdir(os.path.join(REF, "python")):
+        raise SystemExit("set DFTTEST2_REF to the vs-dfttest2 source tree")
 
     O.build()
     plugins = {name: _Recorder(name) for name in

@@ -110,15 +110,23 @@ def test_against_fp64_oracle(B, sosize, tb, dtype, bits, cuda_device):
     print(f"B{B} T{tb} {dtype.__name__}: exact-match vs FP64 {exact:.4f}")
 
 
-def test_unsplittable_plane_is_rejected(cuda_device):
-    """sosize 31 of 32 needs strips of at least 31 blocks, wider than the
-    kernel's strips: the call fails with a clear message instead of leaving
-    strips unfiltered."""
-    rng = np.random.default_rng(5)
-    frames = _frames(rng, 3, 91, 109, np.float32, 32)
-    args = plugin_arguments(ftype=0, sigma=5.0, sbsize=32, sosize=31, tbsize=3)
-    with pytest.raises(_lib.Error, match="no split"):
-        gpu_plane(frames, args, 32)
+@pytest.mark.parametrize("B,sosize,tb,w,h", [(32, 31, 3, 73, 61), (32, 29, 3, 120, 50), (32, 28, 1, 109, 91),
+                                             (32, 26, 3, 300, 40), (16, 15, 3, 71, 53)])
+@pytest.mark.parametrize("dtype,bits", [(np.float32, 32), (np.uint16, 16)])
+def test_high_overlap_matches_fp64(B, sosize, tb, w, h, dtype, bits, cuda_device):
+    """Any block_step in [1, sbsize] is a valid reference argument
+    (nvrtc_source/source.cpp block_step checks).  With 32x32 blocks at sosize
+    26..31 no strip of the kernel's width is O/S blocks wide, so the strips
+    are narrower than the overlap and the fix-up kernel sums every strip that
+    covers a pixel; the result matches the FP64 oracle like any other case."""
+    rng = np.random.default_rng(B + sosize + w)
+    frames = _frames(rng, tb, h, w, dtype, bits)
+    args = plugin_arguments(ftype=0, sigma=5.0, sbsize=B, sosize=sosize, tbsize=tb)
+    f64 = O.fp64_plane(list(frames), args, bits)
+    ref = O.quantize(f64, dtype, bits) if dtype != np.float32 else f64
+    out = gpu_plane(frames, args, bits)
+    exact = check(out, ref, bits, f"B{B} sosize {sosize} T{tb} {w}x{h}")
+    print(f"B{B} sosize {sosize} T{tb}: exact-match vs FP64 {exact:.4f}")
 
 
 def test_device_path_equals_host_path(cuda_device):

@@ -11,7 +11,8 @@ Checked here through the C ABI: two calls in a row, on different inputs,
 each match the regular entry point (dfttest2_b200_process_planes) within the
 parity tolerance of the other GPU tests (1 LSB on integer planes, 2e-5 of
 full scale on float planes); a plane that needs more scratch than the array
-holds is rejected with a clear message.  This file is collected last so that
+holds is rejected with a clear message; the kernels' error word, read by
+dfttest2_b200_noalloc_check, reports no failure.  This file is collected last so that
 a run stopping at the first failure has already run every other test.
 """
 import ctypes
@@ -110,6 +111,9 @@ def test_noalloc_matches_regular_path_twice(fmt, cuda_device):
                                                      ctypes.c_void_p(stream))
         assert rc == 0, lib.dfttest2_b200_last_error().decode()
         outs.append(out)
+    # the kernels' error word (in the same static array) reports no failure
+    rc = lib.dfttest2_b200_noalloc_check(0, ctypes.c_void_p(stream))
+    assert rc == 0, lib.dfttest2_b200_last_error().decode()
     torch.cuda.synchronize()
     for got, want in zip(outs, ref):
         assert _close(got.cpu().numpy(), want, fmt == "f32")
@@ -122,9 +126,11 @@ def test_noalloc_rejects_planes_beyond_the_array(cuda_device):
     args = plugin_arguments(ftype=0, sigma=8.0, sbsize=16, sosize=12, tbsize=3)
     lib = _lib.load()
     p, keep = _params(args)
-    # a 16384 x 8192 float plane needs far more overlap scratch than the array holds;
-    # the check happens before anything touches the pointers
-    big = torch.empty((1, 16), dtype=torch.float32, device=cuda_device)
+    # a 16384 x 8192 float plane needs far more overlap scratch than the array
+    # holds.  The plane is a real allocation of that size (512 MiB) even though
+    # the host-side check rejects the call before any launch: were the check
+    # ever to regress, the kernels would still stay inside allocated memory.
+    big = torch.zeros((8192, 16384), dtype=torch.float32, device=cuda_device)
     pl = _lib.Plane()
     for t in range(3):
         pl.src[t] = big.data_ptr()

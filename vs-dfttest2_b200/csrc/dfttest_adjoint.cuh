@@ -465,14 +465,4 @@ __global__ void __launch_bounds__(256) dfttest_adjoint_kernel(const __grid_const
     }
 }
 
-// builds the gain-slot sigma tables of the forward kernel from a device sigma array
-__global__ void __launch_bounds__(256) sigma_tables_kernel(const float* __restrict__ sigma, const int* __restrict__ idx,
-                                                           const int* __restrict__ idx2, float* __restrict__ tab,
-                                                           float* __restrict__ tab2, int n) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        tab[i] = sigma[idx[i]];
-        tab2[i] = sigma[idx2[i]];
-    }
-}
-
 }  // namespace dft2

@@ -26,9 +26,25 @@
 #include <vector>
 
 #include "dfttest2_b200.h"
-#include "dfttest_kernel.cuh"
-#include "dfttest_adjoint.cuh"
-#include "dfttest_tc.cuh"
+#include "dfttest_host.h"
+
+namespace {
+thread_local std::string g_last_error;
+}  // namespace
+
+int dft2h::fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+dft2h::Variant dft2h::unit_variant(int B, int T, int NW, int MINB) {
+    switch (B) {
+    case 8: return unit_variant_b8(T, NW, MINB);
+    case 16: return unit_variant_b16(T, NW, MINB);
+    case 32: return unit_variant_b32(T, NW, MINB);
+    }
+    return Variant{};
+}
 
 #ifndef DFTTEST2_B200_VERSION
 #define DFTTEST2_B200_VERSION "0.1.0"
@@ -36,46 +52,7 @@
 
 namespace {
 
-thread_local std::string g_last_error;
-
-int fail(int code, const std::string& msg) {
-    g_last_error = msg;
-    return code;
-}
-
-#define CUDA_TRY(expr)                                                                                   \
-    do {                                                                                                 \
-        cudaError_t e_ = (expr);                                                                         \
-        if (e_ != cudaSuccess) {                                                                         \
-            return fail(DFTTEST2_B200_ECUDA, std::string("[") + std::to_string(__LINE__) + "] '" #expr   \
-                                                 "' failed: " + cudaGetErrorString(e_));                 \
-        }                                                                                                \
-    } while (0)
-
-using KernelFn = void (*)(const dft2::KernelArgs);
-
-struct Variant {
-    KernelFn main = nullptr;      // Wiener fast path
-    KernelFn generic = nullptr;   // every filter type, asymmetric sigma
-    KernelFn fixup = nullptr;
-    int nw = 0;      // warps per CTA
-    int bpw = 0;     // blocks per warp
-    int minb = 1;    // CTAs per SM the register budget is sized for
-    size_t (*smem)(int pitch) = nullptr;
-};
-
-template <int B, int T, int NW, int MINB = 1>
-Variant make_variant() {
-    Variant v;
-    v.main = dft2::dfttest_unit_kernel<B, T, NW, dft2::kFilterWiener, MINB>;
-    v.generic = dft2::dfttest_unit_kernel<B, T, NW, dft2::kFilterGeneric, MINB>;
-    v.fixup = dft2::dfttest_fixup_kernel<B>;
-    v.nw = NW;
-    v.bpw = 32 / B;
-    v.minb = MINB;
-    v.smem = [](int pitch) { return dft2::Layout<B, T, NW>::smem_bytes(pitch); };
-    return v;
-}
+using namespace dft2h;
 
 // kernel variants per (block size, temporal size): NW warps per CTA keeps
 // the per-warp block buffers plus the rings within 227 KB of shared memory
@@ -90,39 +67,35 @@ Variant make_variant() {
 Variant select_variant(int B, int T, int S) {
     // DFTTEST2_B200_WARPS=16 / 8 / 4 select other 16x16x3 shapes
     const char* env = std::getenv("DFTTEST2_B200_WARPS");
-    if (env && B == 16 && T == 3 && std::atoi(env) == 16) return make_variant<16, 3, 16>();
-    if (env && B == 16 && T == 3 && std::atoi(env) == 8) return make_variant<16, 3, 8, 2>();
-    if (env && B == 16 && T == 3 && std::atoi(env) == 4) return make_variant<16, 3, 4, 4>();
+    if (env && B == 16 && T == 3 && std::atoi(env) == 16) return unit_variant(16, 3, 16, 1);
+    if (env && B == 16 && T == 3 && std::atoi(env) == 8) return unit_variant(16, 3, 8, 2);
+    if (env && B == 16 && T == 3 && std::atoi(env) == 4) return unit_variant(16, 3, 4, 4);
     switch (B) {
-#ifndef DFTTEST2_B200_ONLY_B16
     case 8:
         switch (T) {
-        case 1: return make_variant<8, 1, 16>();
-        case 3: return make_variant<8, 3, 16>();
-        case 5: return make_variant<8, 5, 16>();
-        case 7: return make_variant<8, 7, 16>();
+        case 1: return unit_variant(8, 1, 16, 1);
+        case 3: return unit_variant(8, 3, 16, 1);
+        case 5: return unit_variant(8, 5, 16, 1);
+        case 7: return unit_variant(8, 7, 16, 1);
         }
         break;
-#endif
     case 16:
         switch (T) {
-        case 1: return make_variant<16, 1, 16>();
-        case 3: return make_variant<16, 3, 10, 2>();
-        case 5: return make_variant<16, 5, 12>();
-        case 7: return make_variant<16, 7, 8>();
+        case 1: return unit_variant(16, 1, 16, 1);
+        case 3: return unit_variant(16, 3, 10, 2);
+        case 5: return unit_variant(16, 5, 12, 1);
+        case 7: return unit_variant(16, 7, 8, 1);
         }
         break;
-#ifndef DFTTEST2_B200_ONLY_B16
     case 32:
         switch (T) {
-        case 1: return make_variant<32, 1, 16>();
+        case 1: return unit_variant(32, 1, 16, 1);
         // two 6-warp CTAs per SM unless the overlap needs wider strips (sosize 26 and up)
-        case 3: return S >= 7 ? make_variant<32, 3, 6, 2>() : make_variant<32, 3, 8>();
-        case 5: return make_variant<32, 5, 5>();
-        case 7: return make_variant<32, 7, 5>();
+        case 3: return S >= 7 ? unit_variant(32, 3, 6, 2) : unit_variant(32, 3, 8, 1);
+        case 5: return unit_variant(32, 5, 5, 1);
+        case 7: return unit_variant(32, 7, 5, 1);
         }
         break;
-#endif
     }
     return Variant{};
 }
@@ -144,20 +117,18 @@ std::vector<Variant> candidate_variants(int B, int T, int S) {
     std::vector<Variant> v;
     v.push_back(select_variant(B, T, S));
     if (!v.back().main) return {};
-#ifndef DFTTEST2_B200_ONLY_B16
-    if (B == 8 && T == 1) v.push_back(make_variant<8, 1, 8, 2>());
-    if (B == 8 && T == 3) v.push_back(make_variant<8, 3, 8, 2>());
-    if (B == 32 && T == 1) v.push_back(make_variant<32, 1, 8>());
+    if (B == 8 && T == 1) v.push_back(unit_variant(8, 1, 8, 2));
+    if (B == 8 && T == 3) v.push_back(unit_variant(8, 3, 8, 2));
+    if (B == 32 && T == 1) v.push_back(unit_variant(32, 1, 8, 1));
     if (B == 32 && T == 3) {
-        v.push_back(S >= 7 ? make_variant<32, 3, 8>() : make_variant<32, 3, 6, 2>());
-        v.push_back(make_variant<32, 3, 4, 2>());
+        v.push_back(S >= 7 ? unit_variant(32, 3, 8, 1) : unit_variant(32, 3, 6, 2));
+        v.push_back(unit_variant(32, 3, 4, 2));
     }
-#endif
-    if (B == 16 && T == 1) v.push_back(make_variant<16, 1, 8, 2>());
+    if (B == 16 && T == 1) v.push_back(unit_variant(16, 1, 8, 2));
     if (B == 16 && T == 3) {
-        v.push_back(make_variant<16, 3, 8, 2>());
-        v.push_back(make_variant<16, 3, 16>());
-        v.push_back(make_variant<16, 3, 4, 4>());
+        v.push_back(unit_variant(16, 3, 8, 2));
+        v.push_back(unit_variant(16, 3, 16, 1));
+        v.push_back(unit_variant(16, 3, 4, 4));
     }
     return v;
 }
@@ -176,7 +147,8 @@ struct Slot {
     size_t scratch_cap = 0;               // floats
     int* d_seams = nullptr;               // seam arrival counters (full-strip launches)
     size_t seams_cap = 0;
-    int* d_error = nullptr;
+    int* d_error = nullptr;               // error word of the slot's kernels (0 = no failure)
+    int* h_error = nullptr;               // pinned copy of d_error read by the host-synchronous paths
     // host path staging
     void* d_frames = nullptr;
     size_t frames_cap = 0;
@@ -222,6 +194,7 @@ struct dfttest2_b200_filter {
     int tc_mode = 0;
     void* d_gmat = nullptr;
     int gmat_bytes = 0;
+    int wait_limit = dft2::kDefaultWaitLimit;  // iteration limit of the kernels' bounded device waits
 
     std::vector<Slot> slots;
     std::vector<int> free_slots;
@@ -345,14 +318,30 @@ struct PlaneRef {
     int param;
 };
 
+// Strips of a plane pnx blocks wide for a kernel of BPS blocks per step:
+// at most BPS blocks each, and at least O/S blocks where possible so that the
+// two edge bands of a strip stay apart (then every overlap seam is shared by
+// exactly two strips).  With high overlap no such split may exist (32x32
+// blocks at sosize 26..31): the strips are then BPS wide and `narrow` is set;
+// their band records hold whole footprints and the fix-up kernel sums every
+// unit that covers a pixel.
+int strip_count(int pnx, int B, int S, int BPS, bool& narrow) {
+    const int O = B - S;
+    const int min_w = (O + S - 1) / S;
+    int nsx = (pnx + BPS - 1) / BPS;
+    while (nsx > 1 && pnx / nsx < min_w) --nsx;
+    narrow = false;
+    if ((pnx + nsx - 1) / nsx > BPS) {
+        nsx = (pnx + BPS - 1) / BPS;
+        narrow = nsx > 1;
+    }
+    return nsx;
+}
+
 // Unit split and work-list of planes that share (B, S) and a kernel shape of
-// BPS blocks per step: strips of at most BPS blocks; each strip is cut into
-// segments until the launch has about `target` units (segments no shorter
-// than max(O/S, 4) blocks).
-// Fails (EINVAL) when some plane has no strip split whose strips are at
-// least O/S blocks wide (so that the two edge bands of a strip stay apart)
-// and at most BPS blocks wide (the kernel's blocks per step); the unit
-// kernel would otherwise skip the wider strips.
+// BPS blocks per step: strips of at most BPS blocks (strip_count); each strip
+// is cut into segments until the launch has about `target` units (segments no
+// shorter than max(O/S, 4) blocks).
 int plan_units(int B, int S, int BPS, const std::vector<PlaneRef>& planes, long long target, Plan& plan) {
     const int O = B - S;
     const int n = (int)planes.size();
@@ -382,21 +371,14 @@ int plan_units(int B, int S, int BPS, const std::vector<PlaneRef>& planes, long 
         j.height = p.height;
         j.param = p.param;
         const int pnx = dft2::pad_num(p.width, B, S), pny = dft2::pad_num(p.height, B, S);
-        j.nsx = (pnx + BPS - 1) / BPS;
+        bool narrow = false;
+        j.nsx = strip_count(pnx, B, S, BPS, narrow);
         j.nsy = std::max(1, std::min(nsy, pny / min_seg));
-        // strips must be at least O/S blocks wide so that bands do not overlap
-        while (j.nsx > 1 && pnx / j.nsx < (O + S - 1) / S) --j.nsx;
-        if ((pnx + j.nsx - 1) / j.nsx > BPS)
-            return fail(DFTTEST2_B200_EINVAL,
-                        "sbsize " + std::to_string(B) + " / sosize " + std::to_string(O) + " on a plane " +
-                            std::to_string(p.width) + " wide: no split into strips of " +
-                            std::to_string((O + S - 1) / S) + " to " + std::to_string(BPS) +
-                            " blocks (use a smaller sosize)");
         j.unit_base = unit;
         j.fix_base = fix;
         j.seam_base = seams;
         seams += j.nsx - 1;
-        full = full && j.nsy == 1;
+        full = full && j.nsy == 1 && !narrow;
         unit += j.nsx * j.nsy;
         fix += (j.nsx - 1) * O * p.height + (j.nsy - 1) * O * p.width;
         const int wmax = (pnx + j.nsx - 1) / j.nsx, hmax = (pny + j.nsy - 1) / j.nsy;
@@ -469,106 +451,6 @@ int make_plan(const dfttest2_b200_filter* f, const dfttest2_b200_plane* planes, 
 }
 
 // ---- tensor-core form ------------------------------------------------------
-using TcKernelFn = void (*)(const dft2::TcArgs);
-
-struct TcVariant {
-    TcKernelFn wiener = nullptr, generic = nullptr;
-    size_t (*smem)(int patch_w) = nullptr;
-    int gbytes = 0;
-    int tb = 0;  // blocks per tile
-    void (*build)(std::vector<char>&) = nullptr;
-};
-
-// the constant operands (N x K, K-major canonical layout) of the four products
-template <int B, int T, int MODE>
-void build_gmat(std::vector<char>& img) {
-    using L = dft2::TcLayout<B, T, MODE>;
-    constexpr int ESZ = L::ESZ;
-    img.assign(L::GBYTES, 0);
-    const double pi = 3.14159265358979323846;
-    auto put = [&](int off, int n, int k, int KT, double v) {
-        const int idx = off + dft2::op_index<ESZ>(n, k, KT);
-        if (MODE == dft2::kTcTf32) {
-            // round to the 10-bit tf32 mantissa, nearest even (the tensor cores would truncate)
-            const float f = (float)v;
-            uint32_t u;
-            std::memcpy(&u, &f, 4);
-            u = (u + 0x0FFFu + ((u >> 13) & 1u)) & ~0x1FFFu;
-            std::memcpy(&img[(size_t)idx * 4], &u, 4);
-        } else {
-            const __nv_bfloat16 h = __float2bfloat16_rn((float)v);
-            std::memcpy(&img[(size_t)idx * 2], &h, 2);
-            if (MODE == dft2::kTcBf16x3) {
-                const __nv_bfloat16 l = __float2bfloat16_rn((float)(v - (double)__bfloat162float(h)));
-                std::memcpy(&img[(size_t)(L::GELEM + idx) * 2], &l, 2);
-            }
-        }
-    };
-    // G1: packed r2c of a row, [j][x]
-    for (int j = 0; j < B; ++j)
-        for (int x = 0; x < B; ++x) {
-            const int k = j < 2 ? (j == 0 ? 0 : B / 2) : j / 2;
-            const double ang = 2.0 * pi * k * x / B;
-            put(L::g1, j, x, B, j < 2 ? std::cos(ang) : ((j & 1) ? -std::sin(ang) : std::cos(ang)));
-        }
-    // G2: forward complex DFT over y in real form, [(c', ky)][(c, y)]
-    for (int cp = 0; cp < 2; ++cp)
-        for (int ky = 0; ky < B; ++ky)
-            for (int c = 0; c < 2; ++c)
-                for (int y = 0; y < B; ++y) {
-                    const double th = 2.0 * pi * (double)(ky * y % B) / B;
-                    const double v = cp == c ? std::cos(th) : (c == 1 ? std::sin(th) : -std::sin(th));
-                    put(L::g2, cp * B + ky, c * B + y, 2 * B, v);
-                }
-    // G4: inverse complex DFT over y, [(c', y)][(c, ky)]
-    for (int cp = 0; cp < 2; ++cp)
-        for (int y = 0; y < B; ++y)
-            for (int c = 0; c < 2; ++c)
-                for (int ky = 0; ky < B; ++ky) {
-                    const double ph = 2.0 * pi * (double)(ky * y % B) / B;
-                    const double v = cp == c ? std::cos(ph) : (c == 1 ? -std::sin(ph) : std::sin(ph));
-                    put(L::g4, cp * B + y, c * B + ky, 2 * B, v);
-                }
-    // G5: c2r of a packed row, [x][j]
-    for (int x = 0; x < B; ++x)
-        for (int j = 0; j < B; ++j) {
-            const int k = j < 2 ? (j == 0 ? 0 : B / 2) : j / 2;
-            const double ang = 2.0 * pi * (double)(k * x % B) / B;
-            put(L::g5, x, j, B, j < 2 ? std::cos(ang) : ((j & 1) ? -2.0 * std::sin(ang) : 2.0 * std::cos(ang)));
-        }
-}
-
-template <int B, int T, int MODE>
-TcVariant make_tc() {
-    TcVariant v;
-    v.wiener = dft2::dfttest_tc_kernel<B, T, MODE, dft2::kFilterWiener>;
-    v.generic = dft2::dfttest_tc_kernel<B, T, MODE, dft2::kFilterGeneric>;
-    v.smem = [](int pw) { return dft2::TcLayout<B, T, MODE>::bytes(pw); };
-    v.gbytes = dft2::TcLayout<B, T, MODE>::GBYTES;
-    v.tb = dft2::TcLayout<B, T, MODE>::TB;
-    v.build = build_gmat<B, T, MODE>;
-    return v;
-}
-
-template <int B, int T>
-TcVariant select_tc_mode(int mode) {
-    switch (mode) {
-    case dft2::kTcBf16x3: return make_tc<B, T, dft2::kTcBf16x3>();
-    case dft2::kTcTf32: return make_tc<B, T, dft2::kTcTf32>();
-    case dft2::kTcBf16: return make_tc<B, T, dft2::kTcBf16>();
-    }
-    return TcVariant{};
-}
-
-TcVariant select_tc(int B, int T, int mode) {
-    if (B == 16 && T == 1) return select_tc_mode<16, 1>(mode);
-    if (B == 16 && T == 3) return select_tc_mode<16, 3>(mode);
-#ifndef DFTTEST2_B200_ONLY_B16
-    if (B == 32 && T == 1) return select_tc_mode<32, 1>(mode);
-#endif
-    return TcVariant{};
-}
-
 int launch_tc(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, float scale, float peak,
               cudaStream_t stream) {
     const TcVariant v = select_tc(f->B, f->T, f->tc_mode);
@@ -622,6 +504,7 @@ int launch_tc(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, f
     a.gmat = f->d_gmat;
     a.gmat_bytes = f->gmat_bytes;
     a.error_flag = slot.d_error;
+    a.wait_limit = f->wait_limit;
     const int patch_w = B + (v.tb - 1) * S;
     const size_t smem = v.smem(patch_w);
     if (smem > 227 * 1024) return fail(DFTTEST2_B200_EINVAL, "block step too large for the tensor-core form");
@@ -638,8 +521,7 @@ int launch_tc(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, f
     CUDA_TRY(cudaGetLastError());
     dim3 fg((unsigned)std::max<long long>(1, std::min<long long>(64, (acc / jobs.size() + 255) / 256)),
             (unsigned)jobs.size());
-    dft2::dfttest_tc_finalize<<<fg, 256, 0, stream>>>(a);
-    CUDA_TRY(cudaGetLastError());
+    if (int rc = launch_tc_finalize(a, fg, stream)) return rc;
     CUDA_TRY(cudaEventRecord(slot.done, stream));
     return 0;
 }
@@ -723,6 +605,112 @@ void centre_first_wf(const double* wf, int t, int T, int r, float& re, float& im
     im = (float)(wf[0] * sn + wf[1] * c);
 }
 
+// Storage for the FP32 tables the unit kernel reads (every pointer holds the
+// capacity for the filter's T, B): analysis window [T][B][B], synthesis
+// window [B][B], and per gain slot [T][B/2+2][B] the sigma, the sigma of the
+// Hermitian partner bin and the window spectrum (re, im).  sig_idx and
+// sig2_idx (may be null) receive the (t, y, x) index of each slot's bin.
+struct TableSpans {
+    float* win;
+    float* wsyn;
+    float* sig;
+    float* sig2;
+    float* wfe;
+    int* sig_idx;
+    int* sig2_idx;
+};
+
+// Builds the tables from the plugin arrays (load_block's window,
+// frequency_filtering's sigma, remove_mean's window_freq:
+// cpu_source/getframe_impl.cpp:137, cpu_source/kernel.hpp:1826-1952).  The
+// gain-slot layout is the column phase's: lane w = 2c + h of a block holds
+// the y-bins k = 2m + h of packed x-column c; column 0 carries x-bins 0 (A)
+// and B/2 (B).  `asym` reports a packed-column bin whose Hermitian partner
+// has a different sigma; `wmask` has bit p set when temporal plane p of the
+// window spectrum is not identically zero.
+void build_tables(const dfttest2_b200_params* p, int B, int radius, bool zero_mean, int syn, const TableSpans& o,
+                  bool& asym, int& wmask) {
+    const int T = 2 * radius + 1, H = B / 2, X = H + 1, M = B / 2, NS = M + 2;
+    for (int i = 0; i < T * B * B; ++i) o.win[i] = (float)p->window[i];
+    for (int i = 0; i < B * B; ++i) o.wsyn[i] = o.win[syn * B * B + i];
+    auto sigma_at = [&](int t, int y, int x) -> float {
+        return p->sigma_len == 1 ? (float)p->sigma[0] : (float)p->sigma[(t * B + y) * X + x];
+    };
+    asym = false;
+    auto put = [&](int pl, int j, int w, int t, int y, int x, int t2, int y2) {
+        const int idx = (pl * NS + j) * B + w;
+        if (o.sig_idx) o.sig_idx[idx] = (t * B + y) * X + x;
+        if (o.sig2_idx) o.sig2_idx[idx] = (t2 * B + y2) * X + x;
+        o.sig[idx] = sigma_at(t, y, x);
+        o.sig2[idx] = sigma_at(t2, y2, x);
+        o.wfe[2 * idx] = o.wfe[2 * idx + 1] = 0.0f;
+        if (zero_mean)
+            centre_first_wf(&p->window_freq[((t * B + y) * X + x) * 2], t, T, radius, o.wfe[2 * idx], o.wfe[2 * idx + 1]);
+        if (o.sig2[idx] != o.sig[idx]) asym = true;
+    };
+    auto neg = [&](int k) { return (B - k) % B; };
+    for (int pl = 0; pl < T; ++pl) {
+        for (int w = 0; w < B; ++w) {
+            const int c = w >> 1, h = w & 1;
+            for (int j = 0; j < NS; ++j) put(pl, j, w, 0, 0, 0, 0, 0);  // unused slots
+            if (c > 0) {
+                for (int m = 0; m < M; ++m) put(pl, m, w, pl, 2 * m + h, c, pl, 2 * m + h);
+                continue;
+            }
+            if (pl > 0) {
+                for (int m = 0; m < M; ++m) {
+                    const int k = 2 * m + h;
+                    if (pl <= radius) put(pl, m, w, pl, k, 0, T - pl, neg(k));
+                    else put(pl, m, w, T - pl, k, H, pl, neg(k));
+                }
+                continue;
+            }
+            // plane 0 of the packed column: untangled A (x-bin 0) and B (x-bin B/2)
+            if (h == 0) {
+                put(0, 0, w, 0, 0, 0, 0, 0);            // A(0)
+                put(0, M / 2, w, 0, H, 0, 0, H);        // A(B/2)
+                for (int m = 1; m < M / 2; ++m) {
+                    put(0, m, w, 0, 2 * m, 0, 0, neg(2 * m));      // A(2m)
+                    put(0, M - m, w, 0, 2 * m, H, 0, neg(2 * m));  // B(2m)
+                }
+                put(0, M, w, 0, 0, H, 0, 0);            // B(0)
+                put(0, M + 1, w, 0, H, H, 0, H);        // B(B/2)
+            } else {
+                for (int m = 0; m < M / 2; ++m) {
+                    put(0, m, w, 0, 2 * m + 1, 0, 0, neg(2 * m + 1));          // A(2m+1)
+                    put(0, M - 1 - m, w, 0, 2 * m + 1, H, 0, neg(2 * m + 1));  // B(2m+1)
+                }
+            }
+        }
+    }
+    // temporal planes whose window spectrum is identically zero skip the
+    // zero-mean terms (every plane but 0 for a rectangular temporal window)
+    wmask = 0;
+    for (int pl = 0; pl < T; ++pl)
+        for (int i = 0; i < NS * B * 2; ++i)
+            if (o.wfe[pl * NS * B * 2 + i] != 0.0f) wmask |= 1 << pl;
+}
+
+// Text of the codes the kernels leave in their error word.
+std::string kernel_error_text(int code) {
+    switch (code) {
+    case 1: return "kernel error 1: a unit's strip is wider than the kernel's blocks per step (planner inconsistency)";
+    case 2: return "kernel error 2: a bounded wait for the tensor cores ran out (no completion signal within the limit)";
+    case 3: return "kernel error 3: a bounds check of the checked build failed (index outside its buffer)";
+    default: return "kernel error " + std::to_string(code);
+    }
+}
+
+// Reads and clears a slot's error word after its stream has been waited for
+// (the caller queued a copy of d_error into h_error before the wait).
+int slot_status(Slot& s) {
+    const int code = *s.h_error;
+    if (code == 0) return 0;
+    *s.h_error = 0;
+    CUDA_TRY(cudaMemset(s.d_error, 0, sizeof(int)));
+    return fail(DFTTEST2_B200_EKERNEL, kernel_error_text(code));
+}
+
 void scale_peak(int sample_type, int bits, float& scale, float& peak, int& kind) {
     if (sample_type == DFTTEST2_B200_FLOAT) {
         scale = 255.0f;
@@ -733,52 +721,6 @@ void scale_peak(int sample_type, int bits, float& scale, float& peak, int& kind)
         peak = (float)((1 << bits) - 1);
         kind = bits <= 8 ? dft2::kU8 : dft2::kU16;
     }
-}
-
-template <int B, int T>
-int launch_adjoint_t(dft2::AdjointArgs a, int num_sms, cudaStream_t st) {
-    using L = dft2::AdjTile<B, T>;
-    a.patch_h = B + (L::TBY - 1) * a.block_step;
-    a.patch_w = B + (L::TBX - 1) * a.block_step;
-    const size_t smem = L::smem_bytes(a.patch_h, a.patch_w);
-    auto kern = dft2::dfttest_adjoint_kernel<B, T>;
-    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, L::NTH, smem));
-    if (per_sm < 1) return fail(DFTTEST2_B200_ECUDA, "adjoint kernel does not fit on an SM");
-    const int grid = std::max(1, std::min(a.ntiles, num_sms * per_sm));
-    kern<<<grid, L::NTH, smem, st>>>(a);
-    CUDA_TRY(cudaGetLastError());
-    return 0;
-}
-
-template <int B, int T>
-void adjoint_tile_dims_t(int& tbx, int& tby) {
-    tbx = dft2::AdjTile<B, T>::TBX;
-    tby = dft2::AdjTile<B, T>::TBY;
-}
-
-#define DFT2_FOR_ADJ_VARIANTS(M) M(16, 1) M(16, 3) M(16, 5) M(16, 7)
-#ifndef DFTTEST2_B200_ONLY_B16
-#define DFT2_FOR_ADJ_MORE(M) M(8, 1) M(8, 3) M(8, 5) M(8, 7) M(32, 1) M(32, 3) M(32, 5) M(32, 7)
-#else
-#define DFT2_FOR_ADJ_MORE(M)
-#endif
-
-int adjoint_tile_dims(int B, int T, int& tbx, int& tby) {
-#define DFT2_ADJ(b, t) \
-    if (B == b && T == t) return adjoint_tile_dims_t<b, t>(tbx, tby), 0;
-    DFT2_FOR_ADJ_VARIANTS(DFT2_ADJ) DFT2_FOR_ADJ_MORE(DFT2_ADJ)
-#undef DFT2_ADJ
-    return fail(DFTTEST2_B200_EINVAL, "unsupported block_size / radius");
-}
-
-int launch_adjoint(int B, int T, const dft2::AdjointArgs& a, int num_sms, cudaStream_t st) {
-#define DFT2_ADJ(b, t) \
-    if (B == b && T == t) return launch_adjoint_t<b, t>(a, num_sms, st);
-    DFT2_FOR_ADJ_VARIANTS(DFT2_ADJ) DFT2_FOR_ADJ_MORE(DFT2_ADJ)
-#undef DFT2_ADJ
-    return fail(DFTTEST2_B200_EINVAL, "unsupported block_size / radius");
 }
 
 void free_filter(dfttest2_b200_filter* f) {
@@ -794,6 +736,7 @@ void free_filter(dfttest2_b200_filter* f) {
         if (s.d_scratch) cudaFree(s.d_scratch);
         if (s.d_seams) cudaFree(s.d_seams);
         if (s.d_error) cudaFree(s.d_error);
+        if (s.h_error) cudaFreeHost(s.h_error);
         if (s.d_frames) cudaFree(s.d_frames);
         if (s.d_sigtab) cudaFree(s.d_sigtab);
         if (s.d_gjobs) cudaFree(s.d_gjobs);
@@ -887,74 +830,18 @@ int dfttest2_b200_create(const dfttest2_b200_params* p, dfttest2_b200_filter** o
     if (!f->var.main) return fail(DFTTEST2_B200_EINVAL, "unsupported block_size / radius");
 
     // -- tables --------------------------------------------------------------
-    std::vector<float> win(T * B * B), wsyn(B * B);
-    for (int i = 0; i < T * B * B; ++i) win[i] = (float)p->window[i];
-    for (int i = 0; i < B * B; ++i) wsyn[i] = win[syn * B * B + i];
+    const int NS = B / 2 + 2;
+    std::vector<float> win(T * B * B), wsyn(B * B), sig(T * NS * B), sig2(T * NS * B), wfe(2 * T * NS * B);
+    std::vector<int> sig_idx(T * NS * B), sig2_idx(T * NS * B);
+    bool asym = false;
+    int wmask = 0;
+    build_tables(p, B, radius, zero_mean, syn,
+                 TableSpans{win.data(), wsyn.data(), sig.data(), sig2.data(), wfe.data(), sig_idx.data(),
+                            sig2_idx.data()},
+                 asym, wmask);
     auto sigma_at = [&](int t, int y, int x) -> float {
         return p->sigma_len == 1 ? (float)p->sigma[0] : (float)p->sigma[(t * B + y) * X + x];
     };
-    auto wf_rot = [&](int t, int y, int x, float& re, float& im) {
-        re = im = 0.0f;
-        if (zero_mean) centre_first_wf(&p->window_freq[((t * B + y) * X + x) * 2], t, T, radius, re, im);
-    };
-    // Gain-slot tables, laid out [plane][slot][lane w = 2c + h] as the column
-    // phase reads them: lane (c, h) holds the y-bins k = 2m + h of packed
-    // x-column c; column 0 carries x-bins 0 (A) and B/2 (B).  sig2 is the
-    // sigma of the Hermitian partner bin (t, -k) of packed-column bins.
-    const int M = B / 2, NS = M + 2;
-    std::vector<float> sig(T * NS * B), sig2(T * NS * B), wfe(2 * T * NS * B);
-    std::vector<int> sig_idx(T * NS * B), sig2_idx(T * NS * B);
-    bool asym = false;
-    auto put = [&](int pl, int j, int w, int t, int y, int x, int t2, int y2) {
-        const int idx = (pl * NS + j) * B + w;
-        sig_idx[idx] = (t * B + y) * X + x;
-        sig2_idx[idx] = (t2 * B + y2) * X + x;
-        sig[idx] = sigma_at(t, y, x);
-        sig2[idx] = sigma_at(t2, y2, x);
-        wf_rot(t, y, x, wfe[2 * idx], wfe[2 * idx + 1]);
-        if (sig2[idx] != sig[idx]) asym = true;
-    };
-    auto neg = [&](int k) { return (B - k) % B; };
-    for (int pl = 0; pl < T; ++pl) {
-        for (int w = 0; w < B; ++w) {
-            const int c = w >> 1, h = w & 1;
-            for (int j = 0; j < NS; ++j) put(pl, j, w, 0, 0, 0, 0, 0);  // unused slots
-            if (c > 0) {
-                for (int m = 0; m < M; ++m) put(pl, m, w, pl, 2 * m + h, c, pl, 2 * m + h);
-                continue;
-            }
-            if (pl > 0) {
-                for (int m = 0; m < M; ++m) {
-                    const int k = 2 * m + h;
-                    if (pl <= radius) put(pl, m, w, pl, k, 0, T - pl, neg(k));
-                    else put(pl, m, w, T - pl, k, H, pl, neg(k));
-                }
-                continue;
-            }
-            // plane 0 of the packed column: untangled A (x-bin 0) and B (x-bin B/2)
-            if (h == 0) {
-                put(0, 0, w, 0, 0, 0, 0, 0);            // A(0)
-                put(0, M / 2, w, 0, H, 0, 0, H);        // A(B/2)
-                for (int m = 1; m < M / 2; ++m) {
-                    put(0, m, w, 0, 2 * m, 0, 0, neg(2 * m));      // A(2m)
-                    put(0, M - m, w, 0, 2 * m, H, 0, neg(2 * m));  // B(2m)
-                }
-                put(0, M, w, 0, 0, H, 0, 0);            // B(0)
-                put(0, M + 1, w, 0, H, H, 0, H);        // B(B/2)
-            } else {
-                for (int m = 0; m < M / 2; ++m) {
-                    put(0, m, w, 0, 2 * m + 1, 0, 0, neg(2 * m + 1));          // A(2m+1)
-                    put(0, M - 1 - m, w, 0, 2 * m + 1, H, 0, neg(2 * m + 1));  // B(2m+1)
-                }
-            }
-        }
-    }
-    // temporal planes whose window spectrum is identically zero skip the
-    // zero-mean terms (every plane but 0 for a rectangular temporal window)
-    int wmask = 0;
-    for (int pl = 0; pl < T; ++pl)
-        for (int i = 0; i < NS * B * 2; ++i)
-            if (wfe[pl * NS * B * 2 + i] != 0.0f) wmask |= 1 << pl;
     f->wmask = wmask;
     f->asym = asym;
     f->g_div = zero_mean ? (float)p->window_freq[0] : 0.0f;
@@ -1007,6 +894,8 @@ int dfttest2_b200_create(const dfttest2_b200_params* p, dfttest2_b200_filter** o
         }
         CUDA_TRY(cudaMalloc((void**)&s.d_error, sizeof(int)));
         CUDA_TRY(cudaMemset(s.d_error, 0, sizeof(int)));
+        CUDA_TRY(cudaMallocHost((void**)&s.h_error, sizeof(int)));
+        *s.h_error = 0;
         CUDA_TRY(cudaEventRecord(s.done, s.stream));
         f->free_slots.push_back(i);
     }
@@ -1042,6 +931,29 @@ int dfttest2_b200_set_precision(dfttest2_b200_filter* f, int mode) {
     CUDA_TRY(cudaMemcpy(f->d_gmat, img.data(), img.size(), cudaMemcpyHostToDevice));
     f->gmat_bytes = (int)img.size();
     f->tc_mode = mode;
+    return 0;
+}
+
+int dfttest2_b200_check(dfttest2_b200_filter* f) {
+    if (!f) return fail(DFTTEST2_B200_EINVAL, "null filter");
+    DeviceGuard dg(f->device);
+    int first = 0;
+    for (Slot& s : f->slots) {
+        CUDA_TRY(cudaEventSynchronize(s.done));
+        int code = 0;
+        CUDA_TRY(cudaMemcpy(&code, s.d_error, sizeof(int), cudaMemcpyDeviceToHost));
+        if (code != 0) {
+            CUDA_TRY(cudaMemset(s.d_error, 0, sizeof(int)));
+            if (!first) first = code;
+        }
+    }
+    if (first) return fail(DFTTEST2_B200_EKERNEL, kernel_error_text(first));
+    return 0;
+}
+
+int dfttest2_b200_set_wait_limit(dfttest2_b200_filter* f, int iterations) {
+    if (!f) return fail(DFTTEST2_B200_EINVAL, "null filter");
+    f->wait_limit = iterations < 0 ? dft2::kDefaultWaitLimit : iterations;
     return 0;
 }
 
@@ -1095,9 +1007,11 @@ int dfttest2_b200_process_plane_host(dfttest2_b200_filter* f, const dfttest2_b20
     int kind;
     scale_peak(sample_type, bits_per_sample, scale, peak, kind);
     if (int rc = launch(f, s, plan, kind, scale, peak, s.stream)) return rc;
+    CUDA_TRY(cudaMemcpyAsync(s.h_error, s.d_error, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
     CUDA_TRY(cudaMemcpyAsync(h + T * frame, dp.dst, frame, cudaMemcpyDeviceToHost, s.stream));
     CUDA_TRY(cudaEventRecord(s.done, s.stream));
     CUDA_TRY(cudaEventSynchronize(s.done));
+    if (int rc = slot_status(s)) return rc;
     uint8_t* dst = (uint8_t*)plane->dst;
     for (int y = 0; y < plane->height; ++y) std::memcpy(dst + y * plane->dst_stride, h + T * frame + y * row, row);
     return 0;
@@ -1255,10 +1169,12 @@ int dfttest2_b200_process_frame_host_cached(dfttest2_b200_filter* f, const dftte
         rc = make_plan(f, dp, nplanes, bps, plan);
         if (rc == 0) rc = launch(f, s, plan, kind, scale, peak, s.stream);
         if (rc == 0) {
-            cudaError_t ce = cudaMemcpyAsync(h_down, s.d_frames, out_total, cudaMemcpyDeviceToHost, s.stream);
+            cudaError_t ce = cudaMemcpyAsync(s.h_error, s.d_error, sizeof(int), cudaMemcpyDeviceToHost, s.stream);
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(h_down, s.d_frames, out_total, cudaMemcpyDeviceToHost, s.stream);
             if (ce == cudaSuccess) ce = cudaEventRecord(s.done, s.stream);
             if (ce == cudaSuccess) ce = cudaEventSynchronize(s.done);
             if (ce != cudaSuccess) rc = fail(DFTTEST2_B200_ECUDA, std::string("filtering failed: ") + cudaGetErrorString(ce));
+            if (rc == 0) rc = slot_status(s);
         }
         if (rc == 0) {
             for (int i = 0; i < nplanes; ++i) {
@@ -1390,10 +1306,11 @@ int dfttest2_b200_process_clip_planes_host(dfttest2_b200_filter* f, const dfttes
         CUDA_TRY(cudaEventRecord(s.ev_down[k & 1], s.down));
         c0 = c1;
     }
+    CUDA_TRY(cudaMemcpyAsync(s.h_error, s.d_error, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
     CUDA_TRY(cudaStreamSynchronize(s.down));
     CUDA_TRY(cudaStreamSynchronize(s.stream));
     CUDA_TRY(cudaEventRecord(s.done, s.stream));
-    return 0;
+    return slot_status(s);
 }
 
 int dfttest2_b200_process_clip_host(dfttest2_b200_filter* f, const void* src, ptrdiff_t src_stride,
@@ -1430,9 +1347,9 @@ int dfttest2_b200_process_planes_sigma(dfttest2_b200_filter* f, const dfttest2_b
     cudaStream_t st = (cudaStream_t)stream;
     CUDA_TRY(cudaStreamWaitEvent(st, s.done, 0));
     if (int rc = ensure(s.d_sigtab, s.sigtab_cap, (size_t)2 * f->n_slots, s.done)) return rc;
-    dft2::sigma_tables_kernel<<<(f->n_slots + 255) / 256, 256, 0, st>>>(sigma, f->d_sig_idx, f->d_sig2_idx, s.d_sigtab,
-                                                                       s.d_sigtab + f->n_slots, f->n_slots);
-    CUDA_TRY(cudaGetLastError());
+    if (int rc = launch_sigma_tables(sigma, f->d_sig_idx, f->d_sig2_idx, s.d_sigtab, s.d_sigtab + f->n_slots,
+                                     f->n_slots, st))
+        return rc;
     return launch(f, s, plan, kind, scale, peak, st, s.d_sigtab, s.d_sigtab + f->n_slots);
 }
 
@@ -1599,7 +1516,11 @@ int noalloc_address(int dev, unsigned char** out) {
 
 size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
-// fixed-capacity tables (T <= 7, B <= 32), built on the host stack
+// Fixed-capacity host tables (T <= 7, B <= 32, about 97 KB): one buffer for
+// the process, not the caller's stack (frame-server worker threads may have
+// small stacks).  g_noalloc_tables_lock is held from the table build until the
+// copies out of the buffer have been queued; copies from pageable memory are
+// staged before cudaMemcpyAsync returns, so the next call may reuse it.
 struct NoAllocTables {
     float win[7 * 32 * 32];
     float wsyn[32 * 32];
@@ -1607,6 +1528,11 @@ struct NoAllocTables {
     float sig2[7 * 18 * 32];
     float wfe[2 * 7 * 18 * 32];
 };
+NoAllocTables g_noalloc_tables;
+std::mutex g_noalloc_tables_lock;
+
+// byte offset of the error word in the array
+constexpr size_t kNoAllocErrorOffset = 0;
 
 }  // namespace
 
@@ -1620,7 +1546,7 @@ extern "C" int dfttest2_b200_process_plane_noalloc(const dfttest2_b200_params* p
     if (B != 8 && B != 16 && B != 32) return fail(DFTTEST2_B200_EINVAL, "\"block_size\" must be 8, 16 or 32");
     const int S = p->block_step < 0 ? B : p->block_step;
     if (S < 1 || S > B) return fail(DFTTEST2_B200_EINVAL, "\"block_step\" must be in [1, block_size]");
-    const int T = 2 * radius + 1, H = B / 2, X = H + 1, M = B / 2, NS = M + 2, O = B - S;
+    const int T = 2 * radius + 1, X = B / 2 + 1, NS = B / 2 + 2, O = B - S;
     const int zero_mean = p->zero_mean < 0 ? 1 : !!p->zero_mean;
     const int device_id = p->device_id < 0 ? 0 : p->device_id;
     if (p->filter_type < 0 || p->filter_type > 6) return fail(DFTTEST2_B200_EINVAL, "\"filter_type\" must be in [0, 6]");
@@ -1635,63 +1561,6 @@ extern "C" int dfttest2_b200_process_plane_noalloc(const dfttest2_b200_params* p
     const Variant var = select_variant(B, T, S);
     if (!var.main) return fail(DFTTEST2_B200_EINVAL, "unsupported block_size / radius");
 
-    // -- tables (same layout as dfttest2_b200_create builds) -----------------
-    NoAllocTables tb;
-    for (int i = 0; i < T * B * B; ++i) tb.win[i] = (float)p->window[i];
-    for (int i = 0; i < B * B; ++i) tb.wsyn[i] = tb.win[syn * B * B + i];
-    auto sigma_at = [&](int t, int y, int x) -> float {
-        return p->sigma_len == 1 ? (float)p->sigma[0] : (float)p->sigma[(t * B + y) * X + x];
-    };
-    auto wf_rot = [&](int t, int y, int x, float& re, float& im) {
-        re = im = 0.0f;
-        if (zero_mean) centre_first_wf(&p->window_freq[((t * B + y) * X + x) * 2], t, T, radius, re, im);
-    };
-    bool asym = false;
-    auto put = [&](int pl, int j, int w, int t, int y, int x, int t2, int y2) {
-        const int idx = (pl * NS + j) * B + w;
-        tb.sig[idx] = sigma_at(t, y, x);
-        tb.sig2[idx] = sigma_at(t2, y2, x);
-        wf_rot(t, y, x, tb.wfe[2 * idx], tb.wfe[2 * idx + 1]);
-        if (tb.sig2[idx] != tb.sig[idx]) asym = true;
-    };
-    auto neg = [&](int k) { return (B - k) % B; };
-    for (int pl = 0; pl < T; ++pl) {
-        for (int w = 0; w < B; ++w) {
-            const int c = w >> 1, h = w & 1;
-            for (int j = 0; j < NS; ++j) put(pl, j, w, 0, 0, 0, 0, 0);
-            if (c > 0) {
-                for (int m = 0; m < M; ++m) put(pl, m, w, pl, 2 * m + h, c, pl, 2 * m + h);
-                continue;
-            }
-            if (pl > 0) {
-                for (int m = 0; m < M; ++m) {
-                    const int k = 2 * m + h;
-                    if (pl <= radius) put(pl, m, w, pl, k, 0, T - pl, neg(k));
-                    else put(pl, m, w, T - pl, k, H, pl, neg(k));
-                }
-                continue;
-            }
-            if (h == 0) {
-                put(0, 0, w, 0, 0, 0, 0, 0);
-                put(0, M / 2, w, 0, H, 0, 0, H);
-                for (int m = 1; m < M / 2; ++m) {
-                    put(0, m, w, 0, 2 * m, 0, 0, neg(2 * m));
-                    put(0, M - m, w, 0, 2 * m, H, 0, neg(2 * m));
-                }
-                put(0, M, w, 0, 0, H, 0, 0);
-                put(0, M + 1, w, 0, H, H, 0, H);
-            } else {
-                for (int m = 0; m < M / 2; ++m) {
-                    put(0, m, w, 0, 2 * m + 1, 0, 0, neg(2 * m + 1));
-                    put(0, M - 1 - m, w, 0, 2 * m + 1, H, 0, neg(2 * m + 1));
-                }
-            }
-        }
-    }
-    int wmask = 0;
-    for (int pl = 0; pl < T; ++pl)
-        for (int i = 0; i < NS * B * 2; ++i)
-            if (tb.wfe[pl * NS * B * 2 + i] != 0.0f) wmask |= 1 << pl;
     const float g_div = zero_mean ? (float)p->window_freq[0] : 0.0f;
     if (zero_mean && g_div == 0.0f) return fail(DFTTEST2_B200_EINVAL, "window_freq[0] must be non-zero");
 
@@ -1716,13 +1585,10 @@ extern "C" int dfttest2_b200_process_plane_noalloc(const dfttest2_b200_params* p
 
     const int BPS = strip_blocks(var, B, S);
     const int pnx = dft2::pad_num(plane->width, B, S), pny = dft2::pad_num(plane->height, B, S);
-    // strips of at least O/S blocks (their edge bands stay apart) and at most BPS
-    int nsx = (pnx + BPS - 1) / BPS;
-    while (nsx > 1 && pnx / nsx < (O + S - 1) / S) --nsx;
-    if ((pnx + nsx - 1) / nsx > BPS)
-        return fail(DFTTEST2_B200_EINVAL, "sosize too large for this sbsize and plane width (no valid strip split)");
+    bool narrow = false;
+    const int nsx = strip_count(pnx, B, S, BPS, narrow);
     const int min_seg = std::max((O + S - 1) / S, 4);
-    const size_t off_err = 0, off_job = 256;
+    const size_t off_err = kNoAllocErrorOffset, off_job = 256;
     const size_t off_win = align256(off_job + sizeof(dft2::PlaneJob));
     const size_t off_wsyn = align256(off_win + sizeof(float) * T * B * B);
     const size_t off_sig = align256(off_wsyn + sizeof(float) * B * B);
@@ -1760,15 +1626,24 @@ extern "C" int dfttest2_b200_process_plane_noalloc(const dfttest2_b200_params* p
     unsigned char* base = nullptr;
     if (int rc = noalloc_address(dev, &base)) return rc;
     cudaStream_t st = (cudaStream_t)stream;
-    // the error flag must start at zero; tables and the descriptor are copied
-    // in (pageable sources are staged before these calls return)
-    CUDA_TRY(cudaMemsetAsync(base + off_err, 0, sizeof(int), st));
-    CUDA_TRY(cudaMemcpyAsync(base + off_job, &job, sizeof(job), cudaMemcpyHostToDevice, st));
-    CUDA_TRY(cudaMemcpyAsync(base + off_win, tb.win, sizeof(float) * T * B * B, cudaMemcpyHostToDevice, st));
-    CUDA_TRY(cudaMemcpyAsync(base + off_wsyn, tb.wsyn, sizeof(float) * B * B, cudaMemcpyHostToDevice, st));
-    CUDA_TRY(cudaMemcpyAsync(base + off_sig, tb.sig, sizeof(float) * T * NS * B, cudaMemcpyHostToDevice, st));
-    CUDA_TRY(cudaMemcpyAsync(base + off_sig2, tb.sig2, sizeof(float) * T * NS * B, cudaMemcpyHostToDevice, st));
-    CUDA_TRY(cudaMemcpyAsync(base + off_wfe, tb.wfe, sizeof(float) * 2 * T * NS * B, cudaMemcpyHostToDevice, st));
+    bool asym = false;
+    int wmask = 0;
+    {
+        // tables as dfttest2_b200_create builds them, in the process-wide host
+        // buffer; the error word must start at zero; tables and descriptor are
+        // copied in (pageable sources are staged before these calls return)
+        std::lock_guard<std::mutex> lk(g_noalloc_tables_lock);
+        NoAllocTables& tb = g_noalloc_tables;
+        build_tables(p, B, radius, zero_mean, syn, TableSpans{tb.win, tb.wsyn, tb.sig, tb.sig2, tb.wfe, nullptr, nullptr},
+                     asym, wmask);
+        CUDA_TRY(cudaMemsetAsync(base + off_err, 0, sizeof(int), st));
+        CUDA_TRY(cudaMemcpyAsync(base + off_job, &job, sizeof(job), cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(base + off_win, tb.win, sizeof(float) * T * B * B, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(base + off_wsyn, tb.wsyn, sizeof(float) * B * B, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(base + off_sig, tb.sig, sizeof(float) * T * NS * B, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(base + off_sig2, tb.sig2, sizeof(float) * T * NS * B, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(base + off_wfe, tb.wfe, sizeof(float) * 2 * T * NS * B, cudaMemcpyHostToDevice, st));
+    }
 
     float scale, peak;
     int kind;
@@ -1809,6 +1684,21 @@ extern "C" int dfttest2_b200_process_plane_noalloc(const dfttest2_b200_params* p
         var.fixup<<<blocks, threads, 0, st>>>(a);
         CUDA_TRY(cudaGetLastError());
     }
+    return 0;
+}
+
+extern "C" int dfttest2_b200_noalloc_check(int device_id, void* stream) {
+    const int dev_id = device_id < 0 ? 0 : device_id;
+    DeviceGuard dg(dev_id);
+    int dev = -1;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev != dev_id) return fail(DFTTEST2_B200_EINVAL, "invalid device_id");
+    unsigned char* base = nullptr;
+    if (int rc = noalloc_address(dev, &base)) return rc;
+    CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    int code = 0;
+    CUDA_TRY(cudaMemcpy(&code, base + kNoAllocErrorOffset, sizeof(int), cudaMemcpyDeviceToHost));
+    if (code != 0) return fail(DFTTEST2_B200_EKERNEL, kernel_error_text(code));
     return 0;
 }
 

@@ -46,6 +46,9 @@ namespace dft2 {
 
 enum SampleKind : int { kU8 = 0, kU16 = 1, kF32 = 2 };
 
+// polls of a bounded device wait before it gives up and reports an error
+constexpr int kDefaultWaitLimit = 1 << 22;
+
 // one output plane of one frame
 struct PlaneJob {
     const void* src[7];   // 2r+1 source planes on the device (time clamp already applied)
@@ -120,9 +123,15 @@ __host__ __device__ inline UnitGeom unit_geom(int sx, int sy, int nsx, int nsy, 
     return u;
 }
 
+// A unit less than 2 O wide or tall (strips narrower than O = B-S, which high
+// overlap forces: 32x32 blocks at sosize 26..31) shares every footprint pixel
+// with a neighbour; its record then holds the whole footprint.
+__host__ __device__ inline bool band_full(int fw, int fh, int O) { return fw < 2 * O || fh < 2 * O; }
+
 // offset of footprint pixel (lx, ly) inside the unit's band record; the band
 // is every footprint pixel within O = B-S of the footprint edge.
 __host__ __device__ inline int band_index(int lx, int ly, int fw, int fh, int O) {
+    if (band_full(fw, fh, O)) return ly * fw + lx;
     if (ly < O) return ly * fw + lx;
     if (ly >= fh - O) return (O + ly - (fh - O)) * fw + lx;
     const int r = ly - O;
@@ -131,7 +140,9 @@ __host__ __device__ inline int band_index(int lx, int ly, int fw, int fh, int O)
     return base + (fh - 2 * O) * O + r * O + (lx - (fw - O));
 }
 
-__host__ __device__ inline int band_record_size(int fw, int fh, int O) { return 2 * O * fw + 2 * (fh - 2 * O) * O; }
+__host__ __device__ inline int band_record_size(int fw, int fh, int O) {
+    return band_full(fw, fh, O) ? fw * fh : 2 * O * fw + 2 * (fh - 2 * O) * O;
+}
 
 __device__ __forceinline__ int mirror(int i, int n) {
     // reflection without edge repeat (cpu_source/getframe_impl.cpp:44-62)

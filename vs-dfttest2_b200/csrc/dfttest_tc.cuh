@@ -56,6 +56,7 @@ struct TcArgs {
     const void* gmat;       // the four constant operands, shared-memory image
     int gmat_bytes;
     int* error_flag;
+    int wait_limit;         // iteration limit of the in-loop waits for the tensor cores
 };
 
 // ---- PTX wrappers (tcgen05, mbarrier) --------------------------------------
@@ -108,10 +109,11 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_addr(bar)), "r"(count) : "memory");
 }
 
-// bounded wait for the phase with the given parity; false when the limit ran out
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// bounded wait for the completion of the phase with the given parity; false
+// when `limit` polls ran out first
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int limit = kDefaultWaitLimit) {
     const uint32_t a = smem_addr(bar);
-    for (int it = 0; it < (1 << 22); ++it) {
+    for (int it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -339,7 +341,7 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc_kernel(const __grid_constan
                 }
             }
             mma_commit(&s_bar);
-            ok = mbar_wait(&s_bar, phase);
+            ok = mbar_wait(&s_bar, phase, a.wait_limit);
             if (!ok) atomicExch(a.error_flag, 2);
         }
         phase ^= 1;
@@ -581,24 +583,14 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc_kernel(const __grid_constan
         }
         // the next tile's first barrier orders these reads before the patch and tile reuse
     }
-    // after a wait that ran out, give the tensor cores one more bounded wait before freeing their memory
-    if (s_fail_any) mbar_wait(&s_bar, phase);
+    // After a wait that ran out, the products of that commit may still be in
+    // flight: wait (with the full limit) for the phase that was being waited
+    // on before freeing the tensor memory they write.  `phase` was already
+    // flipped past it, so that phase's parity is phase ^ 1.
+    if (s_fail_any) mbar_wait(&s_bar, phase ^ 1u);
     tc_fence_before();
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(256) : "memory");
-}
-
-// accumulator planes -> output samples (store_frame, cpu_source/getframe_impl.cpp:177-221)
-__global__ void __launch_bounds__(256) dfttest_tc_finalize(const __grid_constant__ TcArgs a) {
-    const int j = blockIdx.y;
-    const TcJob& job = a.jobs[j];
-    const long long n = (long long)job.width * job.height;
-    const float inv_scale = 1.0f / a.p.scale;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const int y = (int)(i / job.width), x = (int)(i - (long long)y * job.width);
-        store_sample(job.dst, (long long)y * job.dst_stride + x, job.acc[i], a.p.kind, a.p.scale, a.p.peak,
-                     a.p.kind == kF32 ? 0.0f : inv_scale);
-    }
 }
 
 }  // namespace dft2

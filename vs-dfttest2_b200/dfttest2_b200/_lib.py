@@ -126,6 +126,9 @@ SIGNATURES = {
     "dfttest2_b200_process_planes_sigma": (c_int, [c_void_p, POINTER(Plane), c_int, c_int, c_int, c_void_p, c_void_p]),
     "dfttest2_b200_backward_planes": (c_int, [c_void_p, POINTER(GradPlane), c_int, c_void_p, c_void_p, c_void_p]),
     "dfttest2_b200_set_precision": (c_int, [c_void_p, c_int]),
+    "dfttest2_b200_check": (c_int, [c_void_p]),
+    "dfttest2_b200_set_wait_limit": (c_int, [c_void_p, c_int]),
+    "dfttest2_b200_noalloc_check": (c_int, [c_int, c_void_p]),
     "dfttest2_b200_batch_create": (c_int, [POINTER(Clip), c_int, c_int, POINTER(c_void_p)]),
     "dfttest2_b200_batch_run": (c_int, [c_void_p, c_void_p]),
     "dfttest2_b200_batch_describe": (c_int, [c_void_p, ctypes.c_char_p, c_int]),

@@ -75,6 +75,17 @@ class Filter:
         _lib.check(self._lib.dfttest2_b200_set_precision(self.handle, _lib.PRECISION[mode]))
         self.precision = mode
 
+    def check(self) -> None:
+        """Waits for the filter's queued work and raises :class:`Error` if a
+        kernel reported an internal failure (dfttest2_b200_check)."""
+        _lib.check(self._lib.dfttest2_b200_check(self.handle))
+
+    def set_wait_limit(self, iterations: int) -> None:
+        """Iteration limit of the kernels' bounded device waits; negative
+        restores the default (dfttest2_b200_set_wait_limit, for failure-path
+        tests)."""
+        _lib.check(self._lib.dfttest2_b200_set_wait_limit(self.handle, int(iterations)))
+
     def close(self):
         if self.handle:
             self._lib.dfttest2_b200_free(self.handle)
@@ -249,9 +260,7 @@ class _Plugin:
                                                                    fmt.bits_per_sample)):
                     out[p] = o
             if clip.on_gpu:
-                import torch
-
-                torch.cuda.current_stream().synchronize()
+                flt.check()  # waits for the launches; raises if a kernel reported a failure
         finally:
             flt.close()
         return Clip(out, fmt)
