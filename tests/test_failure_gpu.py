@@ -41,7 +41,9 @@ def test_tc_wait_timeout_reports_ekernel_host_path(cuda_device):
         flt.check()
     finally:
         flt.close()
-    assert np.array_equal(good, again)
+    # the tensor-core form sums overlapping blocks with float atomics, whose
+    # order varies from run to run: equal within 1 LSB
+    assert np.abs(good.astype(np.int64) - again.astype(np.int64)).max() <= 1
 
 
 def test_tc_wait_timeout_reports_ekernel_device_path(cuda_device):
@@ -61,7 +63,8 @@ def test_tc_wait_timeout_reports_ekernel_device_path(cuda_device):
         flt.set_wait_limit(-1)
         again = flt.process_clip_device(clip, 0, 16)
         flt.check()
-        assert torch.equal(good, again)
+        d = ((good.to(torch.int32) & 0xFFFF) - (again.to(torch.int32) & 0xFFFF)).abs().max().item()
+        assert d <= 1  # float atomics of the tensor-core form: run-to-run order varies
     finally:
         flt.close()
 
