@@ -24,12 +24,16 @@ struct dfttest2_b200_batch {
         dft2::PlaneJob* d_jobs = nullptr;
         float* d_scratch = nullptr;
         int* d_seams = nullptr;        // seam counters when every unit is a full-height strip
+        void* d_tmaps = nullptr;       // tensor maps of the TMA row staging (null: plain loads)
+        int stage_bw = 0;
+        size_t smem = 0;               // dynamic shared memory of the group's launch
         std::string trials;            // "shape:ms ..." of the tuning runs
         bool cached = false;
     };
     int device = 0;
     int num_sms = 148;
     std::vector<Group> groups;
+    std::vector<int> kinds;            // sample format per clip (FilterParams index)
     dft2::FilterParams* d_params = nullptr;
     int* d_error = nullptr;
     cudaStream_t cap = nullptr;        // capture origin
@@ -53,6 +57,7 @@ void free_batch(dfttest2_b200_batch* b) {
         if (gr.d_jobs) cudaFree(gr.d_jobs);
         if (gr.d_scratch) cudaFree(gr.d_scratch);
         if (gr.d_seams) cudaFree(gr.d_seams);
+        if (gr.d_tmaps) cudaFree(gr.d_tmaps);
     }
     for (cudaStream_t s : b->branch) cudaStreamDestroy(s);
     for (cudaEvent_t e : b->ev) cudaEventDestroy(e);
@@ -79,9 +84,13 @@ int launch_group(const dfttest2_b200_batch* b, const dfttest2_b200_batch::Group&
         CUDA_TRY(cudaMemsetAsync(g.d_seams, 0, (size_t)g.plan.nseams * sizeof(int), st));
         a.seam_count = g.d_seams;
     }
-    const size_t smem = var.smem(g.plan.pitch);
+    if (g.d_tmaps) {
+        a.tmaps = g.d_tmaps;
+        a.stage_bw = g.stage_bw;
+        a.stage_off = (int)((var.smem(g.plan.pitch) + 127) & ~(size_t)127);
+    }
     KernelFn kern = g.generic ? var.generic : var.main;
-    kern<<<g.plan.nunits, var.nw * 32, smem, st>>>(a);
+    kern<<<g.plan.nunits, var.nw * 32, g.smem, st>>>(a);
     CUDA_TRY(cudaGetLastError());
     if (g.plan.nfix > 0 && !g.d_seams) {
         const int threads = 256;
@@ -100,16 +109,37 @@ int prepare_group(dfttest2_b200_batch* b, dfttest2_b200_batch::Group& g, int var
     if (int rc = plan_units(g.B, g.S, strip_blocks(var, g.B, g.S), g.planes, (long long)target_mult * b->num_sms,
                             g.plan))
         return rc;
-    const size_t smem = var.smem(g.plan.pitch);
+    size_t smem = var.smem(g.plan.pitch);
     if (smem > 227 * 1024) return fail(DFTTEST2_B200_EINVAL, "block step too large for the kernel's shared memory");
+    // TMA staging of the input rows where the planes allow it
+    std::vector<int> kinds(g.plan.jobs.size());
+    for (size_t i = 0; i < kinds.size(); ++i) kinds[i] = b->kinds[g.plan.jobs[i].param];
+    std::vector<CUtensorMap> maps;
+    size_t stage = 0;
+    build_stage_maps(g.plan.jobs, kinds, g.B, g.S, g.T, g.plan.pitch, maps, g.stage_bw, stage);
+    if (g.stage_bw > 0 && ((smem + 127) & ~(size_t)127) + stage <= 227 * 1024) {
+        smem = ((smem + 127) & ~(size_t)127) + stage;
+    } else {
+        g.stage_bw = 0;
+        maps.clear();
+        for (auto& j : g.plan.jobs)
+            for (int t = 0; t < 7; ++t) j.tmap[t] = -1;
+    }
+    g.smem = smem;
     KernelFn kern = g.generic ? var.generic : var.main;
     CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (g.d_jobs) CUDA_TRY(cudaFree(g.d_jobs));
     if (g.d_scratch) CUDA_TRY(cudaFree(g.d_scratch));
     if (g.d_seams) CUDA_TRY(cudaFree(g.d_seams));
+    if (g.d_tmaps) CUDA_TRY(cudaFree(g.d_tmaps));
     g.d_jobs = nullptr;
     g.d_scratch = nullptr;
     g.d_seams = nullptr;
+    g.d_tmaps = nullptr;
+    if (!maps.empty()) {
+        CUDA_TRY(cudaMalloc(&g.d_tmaps, maps.size() * sizeof(CUtensorMap)));
+        CUDA_TRY(cudaMemcpy(g.d_tmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+    }
     if (g.plan.nfix > 0 && g.plan.full_strips && g.plan.nseams > 0)
         CUDA_TRY(cudaMalloc((void**)&g.d_seams, (size_t)g.plan.nseams * sizeof(int)));
     CUDA_TRY(cudaMalloc((void**)&g.d_jobs, g.plan.jobs.size() * sizeof(dft2::PlaneJob)));
@@ -228,6 +258,7 @@ int dfttest2_b200_batch_create(const dfttest2_b200_clip* clips, int nclips, int 
         dft2::FilterParams& p = params[c];
         std::memset(&p, 0, sizeof(p));
         p.kind = kind;
+        b->kinds.push_back(kind);
         p.scale = scale;
         p.peak = peak;
         p.filter_type = f->filter_type;

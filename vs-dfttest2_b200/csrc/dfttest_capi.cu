@@ -8,6 +8,8 @@
 //   * splitting every plane into units, sizing the per-unit scratch,
 //   * stream slots for concurrent callers (nvrtc_source/source.cpp:272-291),
 //   * the host-memory paths and RDFT (cpu_source/source.cpp:269-340).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -21,6 +23,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <unordered_map>
 #include <string>
 #include <utility>
 #include <vector>
@@ -133,6 +136,26 @@ std::vector<Variant> candidate_variants(int B, int T, int S) {
     return v;
 }
 
+// Encoded tensor maps kept across launches (a slot's launches reuse its
+// frame buffers): key = (plane pointer, width, height, stride, format, box).
+struct MapKey {
+    const void* p;
+    int w, h, kind, box;
+    long long stride;
+    bool operator==(const MapKey& o) const {
+        return p == o.p && w == o.w && h == o.h && kind == o.kind && box == o.box && stride == o.stride;
+    }
+};
+struct MapKeyHash {
+    size_t operator()(const MapKey& k) const {
+        size_t h = std::hash<const void*>()(k.p);
+        for (long long v : {(long long)k.w, (long long)k.h, (long long)k.kind, (long long)k.box, k.stride})
+            h = h * 1000003u ^ std::hash<long long>()(v);
+        return h;
+    }
+};
+using MapCache = std::unordered_map<MapKey, CUtensorMap, MapKeyHash>;
+
 struct Slot {
     cudaEvent_t done = nullptr;
     cudaStream_t stream = nullptr;        // own stream (host paths)
@@ -147,6 +170,9 @@ struct Slot {
     size_t scratch_cap = 0;               // floats
     int* d_seams = nullptr;               // seam arrival counters (full-strip launches)
     size_t seams_cap = 0;
+    void* d_tmaps = nullptr;              // tensor maps of the TMA row staging
+    size_t tmaps_cap = 0;
+    MapCache map_cache;                   // encoded tensor maps of earlier launches
     int* d_error = nullptr;               // error word of the slot's kernels (0 = no failure)
     int* h_error = nullptr;               // pinned copy of d_error read by the host-synchronous paths
     // host path staging
@@ -363,7 +389,10 @@ int plan_units(int B, int S, int BPS, const std::vector<PlaneRef>& planes, long 
         const PlaneRef& p = planes[i];
         dft2::PlaneJob& j = plan.jobs[i];
         std::memset(&j, 0, sizeof(j));
-        for (int t = 0; t < 7; ++t) j.src[t] = p.src[t];
+        for (int t = 0; t < 7; ++t) {
+            j.src[t] = p.src[t];
+            j.tmap[t] = -1;
+        }
         j.dst = p.dst;
         j.src_stride = p.src_stride;
         j.dst_stride = p.dst_stride;
@@ -526,6 +555,108 @@ int launch_tc(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, f
     return 0;
 }
 
+// ---- TMA staging of the unit kernel's input rows ---------------------------
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+        }
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// Tensor maps for the TMA staging of a launch: one 2D map (width x height
+// samples, rows `stride` bytes apart, box bw x 1) per distinct source plane;
+// jobs[i].tmap[t] indexes them.  kinds[i] is job i's sample format.  A job
+// keeps tmap -1 (staged by plain loads) when its planes break the copy
+// engine's rules (16-byte aligned base and stride, plane at least bw wide) or
+// when some unit of it would read a mirrored column outside the box.  bw = 0
+// (no staging) when the box would exceed 256 samples, no job qualifies, or
+// DFTTEST2_B200_TMA=0.  bw is a multiple of 16 samples, valid for every
+// format; `stage` receives the staging bytes the kernel needs (both slots,
+// widest format) plus 128 for alignment.
+
+void build_stage_maps(std::vector<dft2::PlaneJob>& jobs, const std::vector<int>& kinds, int B, int S, int T,
+                      int pitch, std::vector<CUtensorMap>& maps, int& bw, size_t& stage, MapCache* cache = nullptr) {
+    maps.clear();
+    bw = 0;
+    stage = 0;
+    for (auto& j : jobs)
+        for (int t = 0; t < 7; ++t) j.tmap[t] = -1;
+    const char* env = std::getenv("DFTTEST2_B200_TMA");
+    if (env && std::atoi(env) == 0) return;
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return;
+    const int box = ((pitch + 15) + 15) / 16 * 16;  // footprint + alignment slack of the narrowest format
+    if (box > 256) return;
+    const int O = B - S;
+    if (cache && cache->size() > 8192) cache->clear();
+    std::unordered_map<MapKey, int, MapKeyHash> index;  // this launch's maps
+    for (size_t ji = 0; ji < jobs.size(); ++ji) {
+        dft2::PlaneJob& j = jobs[ji];
+        const int kind = kinds[ji];
+        const int esz = kind == dft2::kF32 ? 4 : (kind == dft2::kU16 ? 2 : 1);
+        const int al = 16 / esz;
+        const long long sb = j.src_stride * esz;
+        bool ok = sb % 16 == 0 && j.width >= box && sb < (1LL << 40);
+        // every unit's footprint columns (mirrored ones included) inside its box, as the kernel checks
+        const int pw = dft2::pad_size(j.width, B, S), pnx = dft2::pad_num(j.width, B, S);
+        const int ox = (pw - j.width) / 2;
+        for (int sx = 0; sx < j.nsx && ok; ++sx) {
+            const int bx0 = dft2::split_lo(sx, pnx, j.nsx), bx1 = dft2::split_lo(sx + 1, pnx, j.nsx);
+            const int x0 = bx0 * S, rowlen = (bx1 - bx0) * S + O;
+            const int xa = (x0 - ox) >= 0 ? ((x0 - ox) / al) * al : -(((ox - x0) + al - 1) / al) * al;
+            const int c_lo = x0 - ox, c_hi = x0 - ox + rowlen - 1;
+            int need_lo = std::max(c_lo, 0), need_hi = std::min(c_hi, j.width - 1);
+            if (c_lo < 0) need_hi = std::max(need_hi, -c_lo);
+            if (c_hi >= j.width) need_lo = std::min(need_lo, 2 * (j.width - 1) - c_hi);
+            ok = need_lo >= xa && need_hi < xa + box && need_lo >= 0 && need_hi < j.width;
+        }
+        int idx[7];
+        const CUtensorMapDataType dt = kind == dft2::kF32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                       : kind == dft2::kU16 ? CU_TENSOR_MAP_DATA_TYPE_UINT16
+                                                            : CU_TENSOR_MAP_DATA_TYPE_UINT8;
+        for (int t = 0; t < T && ok; ++t) {
+            ok = (reinterpret_cast<uintptr_t>(j.src[t]) & 15) == 0;
+            if (!ok) break;
+            const MapKey key{j.src[t], j.width, j.height, kind, box, sb};
+            auto it = index.find(key);
+            if (it == index.end()) {
+                CUtensorMap m;
+                auto hit = cache ? cache->find(key) : MapCache::iterator();
+                if (cache && hit != cache->end()) {
+                    m = hit->second;
+                } else {
+                    const cuuint64_t dims[2] = {(cuuint64_t)j.width, (cuuint64_t)j.height};
+                    const cuuint64_t strides[1] = {(cuuint64_t)sb};
+                    const cuuint32_t boxd[2] = {(cuuint32_t)box, 1u};
+                    const cuuint32_t estr[2] = {1u, 1u};
+                    if (enc(&m, dt, 2, const_cast<void*>(j.src[t]), dims, strides, boxd, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+                        ok = false;
+                        break;
+                    }
+                    if (cache) cache->emplace(key, m);
+                }
+                it = index.emplace(key, (int)maps.size()).first;
+                maps.push_back(m);
+            }
+            idx[t] = it->second;
+        }
+        for (int t = 0; t < 7; ++t) j.tmap[t] = (ok && t < T) ? idx[t] : -1;
+    }
+    if (maps.empty()) return;
+    bw = box;
+    stage = (size_t)dft2::stage_bytes(bw, 4, T, S) + 128;
+}
+
 int launch(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, float scale, float peak,
            cudaStream_t stream, const float* sig_override = nullptr, const float* sig2_override = nullptr) {
     if (plan.nunits == 0) return 0;
@@ -534,8 +665,33 @@ int launch(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, floa
     if (int rc = ensure(slot.d_jobs, slot.jobs_cap, plan.jobs.size(), slot.done)) return rc;
     const size_t scratch_need = (size_t)plan.nunits * plan.rec_stride;
     if (int rc = ensure(slot.d_scratch, slot.scratch_cap, scratch_need, slot.done)) return rc;
-    CUDA_TRY(cudaMemcpyAsync(slot.d_jobs, plan.jobs.data(), plan.jobs.size() * sizeof(dft2::PlaneJob),
-                             cudaMemcpyHostToDevice, stream));
+    // input rows staged by TMA where the planes allow it (within the shared-memory budget)
+    std::vector<dft2::PlaneJob> jobs(plan.jobs);
+    std::vector<CUtensorMap> maps;
+    int bw = 0;
+    size_t stage = 0;
+    const size_t smem_base = f->var.smem(plan.pitch);
+    build_stage_maps(jobs, std::vector<int>(jobs.size(), kind), f->B, f->S, f->T, plan.pitch, maps, bw, stage,
+                     &slot.map_cache);
+    size_t smem = smem_base;
+    if (bw > 0) {
+        const size_t with_stage = ((smem_base + 127) & ~(size_t)127) + stage;
+        if (with_stage <= 227 * 1024) {
+            smem = with_stage;
+        } else {
+            bw = 0;
+            for (auto& j : jobs)
+                for (int t = 0; t < 7; ++t) j.tmap[t] = -1;
+        }
+    }
+    if (bw > 0) {
+        if (int rc = ensure_bytes(slot.d_tmaps, slot.tmaps_cap, maps.size() * sizeof(CUtensorMap), slot.done))
+            return rc;
+        CUDA_TRY(cudaMemcpyAsync(slot.d_tmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice,
+                                 stream));
+    }
+    CUDA_TRY(cudaMemcpyAsync(slot.d_jobs, jobs.data(), jobs.size() * sizeof(dft2::PlaneJob), cudaMemcpyHostToDevice,
+                             stream));
 
     dft2::KernelArgs a{};
     a.jobs = slot.d_jobs;
@@ -569,7 +725,11 @@ int launch(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, floa
         a.seam_count = slot.d_seams;
     }
 
-    const size_t smem = f->var.smem(plan.pitch);
+    if (bw > 0) {
+        a.tmaps = slot.d_tmaps;
+        a.stage_bw = bw;
+        a.stage_off = (int)((smem_base + 127) & ~(size_t)127);
+    }
     KernelFn kern = (f->filter_type == 0 && !f->asym && !sig_override) ? f->var.main : f->var.generic;
     CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<plan.nunits, f->var.nw * 32, smem, stream>>>(a);
@@ -697,6 +857,7 @@ std::string kernel_error_text(int code) {
     case 1: return "kernel error 1: a unit's strip is wider than the kernel's blocks per step (planner inconsistency)";
     case 2: return "kernel error 2: a bounded wait for the tensor cores ran out (no completion signal within the limit)";
     case 3: return "kernel error 3: a bounds check of the checked build failed (index outside its buffer)";
+    case 4: return "kernel error 4: a bounded wait for the TMA copies of input rows ran out";
     default: return "kernel error " + std::to_string(code);
     }
 }
@@ -735,6 +896,7 @@ void free_filter(dfttest2_b200_filter* f) {
         if (s.d_jobs) cudaFree(s.d_jobs);
         if (s.d_scratch) cudaFree(s.d_scratch);
         if (s.d_seams) cudaFree(s.d_seams);
+        if (s.d_tmaps) cudaFree(s.d_tmaps);
         if (s.d_error) cudaFree(s.d_error);
         if (s.h_error) cudaFreeHost(s.h_error);
         if (s.d_frames) cudaFree(s.d_frames);
@@ -1612,6 +1774,7 @@ extern "C" int dfttest2_b200_process_plane_noalloc(const dfttest2_b200_params* p
 
     dft2::PlaneJob job;
     std::memset(&job, 0, sizeof(job));
+    for (int t = 0; t < 7; ++t) job.tmap[t] = -1;  // staged by plain loads
     for (int t = 0; t < T; ++t) job.src[t] = plane->src[t];
     job.dst = plane->dst;
     job.src_stride = plane->src_stride / bps;

@@ -49,6 +49,48 @@ enum SampleKind : int { kU8 = 0, kU16 = 1, kF32 = 2 };
 // polls of a bounded device wait before it gives up and reports an error
 constexpr int kDefaultWaitLimit = 1 << 22;
 
+// ---- PTX wrappers: shared-memory mbarriers and TMA tile loads ---------------
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+// bounded wait for the completion of the phase with the given parity; false
+// when `limit` polls ran out first
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int limit = kDefaultWaitLimit) {
+    const uint32_t a = smem_addr(bar);
+    for (int it = 0; it < limit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done) : "r"(a), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// arrive on the barrier, announcing `bytes` of asynchronous copies that will complete its phase
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+// TMA load of one box of a 2D tensor map (in global memory, 64-byte aligned)
+// at element coordinates (x, y) into shared memory, completing on `bar`.  No
+// cluster multicast: the map covers this GPU's own memory.
+__device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        :: "r"(smem_addr(dst)), "l"(tmap), "r"(x), "r"(y), "r"(smem_addr(bar)) : "memory");
+}
+
+// generic-proxy accesses of this thread to shared memory are ordered before
+// its later asynchronous-proxy (TMA) accesses
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
 // one output plane of one frame
 struct PlaneJob {
     const void* src[7];   // 2r+1 source planes on the device (time clamp already applied)
@@ -61,6 +103,7 @@ struct PlaneJob {
     int fix_base;         // first global fix-up pixel id of this job
     int param;            // index into KernelArgs::params (batched launches)
     int seam_base;        // first seam counter of this job (KernelArgs::seam_count)
+    int tmap[7];          // tensor map of src[t] in KernelArgs::tmaps; -1: rows staged by plain loads
 };
 
 // sample format and filter of a plane: launch-wide, or per job in a batch
@@ -97,7 +140,21 @@ struct KernelArgs {
     // launch; the second strip to finish sums the seam, and no fix-up kernel
     // runs.  Null: the fix-up kernel sums the shared pixels.
     int* seam_count;
+    // TMA staging of input rows: 2D tensor maps (CUtensorMap, 128 bytes each,
+    // one row high and stage_bw samples wide) of the jobs' source planes, and
+    // the byte offset of the two staging slots in dynamic shared memory.
+    // Null: every job is staged by plain loads.
+    const void* tmaps;
+    int stage_bw;
+    int stage_off;
 };
+
+constexpr int kTmapBytes = 128;
+
+// bytes of one staged row (a TMA destination starts on a 128-byte boundary)
+__host__ __device__ inline int stage_row_bytes(int bw, int esz) { return (bw * esz + 127) & ~127; }
+// both staging slots: T planes x S rows each
+__host__ __device__ inline int stage_bytes(int bw, int esz, int T, int S) { return 2 * T * S * stage_row_bytes(bw, esz); }
 
 __host__ __device__ inline int pad_size(int n, int B, int S) {
     return n + ((n % B) ? B - n % B : 0) + 2 * (B - S > S ? B - S : S);
@@ -186,6 +243,71 @@ __device__ __forceinline__ void store_sample(void* base, long long idx, float ac
         reinterpret_cast<uint8_t*>(base)[idx] = (uint8_t)q;
     else
         reinterpret_cast<uint16_t*>(base)[idx] = (uint16_t)q;
+}
+
+// samples of a staged row (raw format) as FP32: four from element e0 (a
+// multiple of 4), or one
+__device__ __forceinline__ float4 stage_load4(const unsigned char* row, int e0, int kind) {
+    if (kind == kF32) return *reinterpret_cast<const float4*>(row + 4 * e0);
+    if (kind == kU16) {
+        const uint2 v = *reinterpret_cast<const uint2*>(row + 2 * e0);
+        return make_float4((float)(v.x & 0xFFFFu), (float)(v.x >> 16), (float)(v.y & 0xFFFFu), (float)(v.y >> 16));
+    }
+    const unsigned v = *reinterpret_cast<const unsigned*>(row + e0);
+    return make_float4((float)(v & 0xFFu), (float)((v >> 8) & 0xFFu), (float)((v >> 16) & 0xFFu), (float)(v >> 24));
+}
+__device__ __forceinline__ float stage_load1(const unsigned char* row, int e, int kind) {
+    if (kind == kF32) return reinterpret_cast<const float*>(row)[e];
+    if (kind == kU16) return (float)reinterpret_cast<const uint16_t*>(row)[e];
+    return (float)row[e];
+}
+
+// Four consecutive output samples (a segment of the overlap-add) with the
+// conversion of store_sample; one vector store where the address is aligned
+// to the four samples (rows of 8 B / 16 B multiples), else scalar stores.
+__device__ __forceinline__ void store4(void* base, long long idx, float4 a, int kind, float peak, float inv_scale) {
+    if (kind == kF32) {
+        // float output: acc / 255 (inv_scale is 0 for float: IEEE division as store_sample)
+        float4 v = make_float4(__fdiv_rn(a.x, 255.0f), __fdiv_rn(a.y, 255.0f), __fdiv_rn(a.z, 255.0f),
+                               __fdiv_rn(a.w, 255.0f));
+        float* p = reinterpret_cast<float*>(base) + idx;
+        if ((reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+            *reinterpret_cast<float4*>(p) = v;
+        } else {
+            p[0] = v.x;
+            p[1] = v.y;
+            p[2] = v.z;
+            p[3] = v.w;
+        }
+        return;
+    }
+    const int pk = (int)peak;
+    auto q = [&](float x) {
+        int v = __float2int_rz(__fadd_rn(x * inv_scale, 0.5f));
+        return v < 0 ? 0 : (v > pk ? pk : v);
+    };
+    const unsigned q0 = q(a.x), q1 = q(a.y), q2 = q(a.z), q3 = q(a.w);
+    if (kind == kU16) {
+        uint16_t* p = reinterpret_cast<uint16_t*>(base) + idx;
+        if ((reinterpret_cast<uintptr_t>(p) & 7) == 0) {
+            *reinterpret_cast<uint2*>(p) = make_uint2(q0 | (q1 << 16), q2 | (q3 << 16));
+        } else {
+            p[0] = (uint16_t)q0;
+            p[1] = (uint16_t)q1;
+            p[2] = (uint16_t)q2;
+            p[3] = (uint16_t)q3;
+        }
+    } else {
+        uint8_t* p = reinterpret_cast<uint8_t*>(base) + idx;
+        if ((reinterpret_cast<uintptr_t>(p) & 3) == 0) {
+            *reinterpret_cast<unsigned*>(p) = q0 | (q1 << 8) | (q2 << 16) | (q3 << 24);
+        } else {
+            p[0] = (uint8_t)q0;
+            p[1] = (uint8_t)q1;
+            p[2] = (uint8_t)q2;
+            p[3] = (uint8_t)q3;
+        }
+    }
 }
 
 // reciprocal from the MUFU unit (PTX rcp.approx.ftz.f32, < 1 ulp)
@@ -536,16 +658,66 @@ template <int M> __device__ __forceinline__ void half_dft_inv(float (&re)[M], fl
 }
 
 // gain of the M bins a lane holds; slot tables are [NSLOT][B] per plane
-template <int M, int B, int FC, bool ZM, bool G>
-__device__ __forceinline__ void gain_lane_zm(float (&re)[M], float (&im)[M], const float* __restrict__ sig,
+// the gain of the general filter class with the filter type fixed (type 0
+// with IEEE division, as gain_rt), for the partner-sigma average of `dual`
+template <int FT, bool ZM>
+__device__ __forceinline__ void apply_bin_ft(float& re, float& im, float s, float s2, bool dual, float2 w, float g,
+                                             const FilterParams& a) {
+    const float dre = ZM ? fmaf(-g, w.x, re) : re;
+    const float dim = ZM ? fmaf(-g, w.y, im) : im;
+    const float psd = fmaf(dim, dim, dre * dre);
+    auto gx = [&](float sg) {
+        if constexpr (FT == 0) return fmaxf(__fdiv_rn(psd - sg, psd + 1e-15f), 0.0f);
+        else return gain<FT>(psd, sg, a);
+    };
+    float m = gx(s);
+    if (dual) m = 0.5f * (m + gx(s2));
+    if constexpr (ZM) {
+        re = fmaf(m, dre, re - dre);
+        im = fmaf(m, dim, im - dim);
+    } else {
+        re *= m;
+        im *= m;
+    }
+}
+
+template <int M, int B, int FT, bool ZM, bool G>
+__device__ __forceinline__ void gain_lane_ft(float (&re)[M], float (&im)[M], const float* __restrict__ sig,
                                              const float* __restrict__ sig2, const float* __restrict__ wfe, int w,
                                              float g, bool dual, const FilterParams& a) {
 #pragma unroll
     for (int j = 0; j < M; ++j) {
         const float s = ldt<G>(sig + j * B + w);
-        const float s2 = (FC != kFilterWiener && dual) ? ldt<G>(sig2 + j * B + w) : s;
+        const float s2 = dual ? ldt<G>(sig2 + j * B + w) : s;
         const float2 wv = ZM ? ldt2<G>(wfe + 2 * (j * B + w)) : make_float2(0.0f, 0.0f);
-        apply_bin<FC, ZM>(re[j], im[j], s, s2, dual, wv, g, a);
+        apply_bin_ft<FT, ZM>(re[j], im[j], s, s2, dual, wv, g, a);
+    }
+}
+
+template <int M, int B, int FC, bool ZM, bool G>
+__device__ __forceinline__ void gain_lane_zm(float (&re)[M], float (&im)[M], const float* __restrict__ sig,
+                                             const float* __restrict__ sig2, const float* __restrict__ wfe, int w,
+                                             float g, bool dual, const FilterParams& a) {
+    if constexpr (FC == kFilterWiener) {
+#pragma unroll
+        for (int j = 0; j < M; ++j) {
+            const float s = ldt<G>(sig + j * B + w);
+            const float2 wv = ZM ? ldt2<G>(wfe + 2 * (j * B + w)) : make_float2(0.0f, 0.0f);
+            apply_bin<FC, ZM>(re[j], im[j], s, s, false, wv, g, a);
+        }
+    } else {
+        // the filter type is uniform: one switch around the bins keeps the
+        // executed code a single straight run (a switch per bin interleaves
+        // all seven gains in the instruction stream)
+        switch (a.filter_type) {
+        case 0: gain_lane_ft<M, B, 0, ZM, G>(re, im, sig, sig2, wfe, w, g, dual, a); break;
+        case 1: gain_lane_ft<M, B, 1, ZM, G>(re, im, sig, sig2, wfe, w, g, dual, a); break;
+        case 2: gain_lane_ft<M, B, 2, ZM, G>(re, im, sig, sig2, wfe, w, g, dual, a); break;
+        case 3: gain_lane_ft<M, B, 3, ZM, G>(re, im, sig, sig2, wfe, w, g, dual, a); break;
+        case 4: gain_lane_ft<M, B, 4, ZM, G>(re, im, sig, sig2, wfe, w, g, dual, a); break;
+        case 5: gain_lane_ft<M, B, 5, ZM, G>(re, im, sig, sig2, wfe, w, g, dual, a); break;
+        default: gain_lane_ft<M, B, 6, ZM, G>(re, im, sig, sig2, wfe, w, g, dual, a); break;
+        }
     }
 }
 
@@ -772,6 +944,31 @@ __device__ __forceinline__ void inverse_row_task(float* __restrict__ wb, const f
 
 __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
+// Plain-load staging of input rows [r_lo, r_lo + nr) of every temporal frame
+// of a unit into the FP32 input ring (mirror padding by index math).  Used for
+// a unit's first B rows, and for every step of units whose planes the TMA
+// copies cannot take; kept out of line so that the unit kernel's step loop
+// stays compact.
+struct StageGeom {
+    const void* const* src;  // the job's 2r+1 source planes
+    long long src_stride;
+    int kind, rowlen, pitch, x0, ox, oy, W, H;
+};
+template <int B, int T, int NT>
+__device__ __noinline__ void stage_rows_plain(float* __restrict__ s_in, const StageGeom g, int r_lo, int nr, int tid) {
+    const float inv_rl = 1.0f / (float)g.rowlen;
+    const float inv_nr_rl = 1.0f / (float)(nr * g.rowlen);
+    for (int i = tid; i < T * nr * g.rowlen; i += NT) {
+        const int t = div_small(i, inv_nr_rl);
+        const int rem = i - t * nr * g.rowlen;
+        const int r = div_small(rem, inv_rl);
+        const int lx = rem - r * g.rowlen;
+        const int py = r_lo + r;
+        const long long gidx = (long long)mirror(py - g.oy, g.H) * g.src_stride + mirror(g.x0 + lx - g.ox, g.W);
+        s_in[(t * B + (py & (B - 1))) * g.pitch + lx] = load_sample(g.src[t], gidx, g.kind);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // main kernel
 // ---------------------------------------------------------------------------
@@ -804,12 +1001,19 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
     __shared__ PlaneJob s_job;
     // and so are its format and filter
     __shared__ FilterParams s_par;
-    static_assert(sizeof(PlaneJob) / sizeof(int) <= 32 && sizeof(FilterParams) / sizeof(int) <= 32, "descriptor size");
-    if (tid < (int)(sizeof(PlaneJob) / sizeof(int)))
-        reinterpret_cast<int*>(&s_job)[tid] = reinterpret_cast<const int*>(&a.jobs[lo])[tid];
-    if (tid >= 32 && tid < 32 + (int)(sizeof(FilterParams) / sizeof(int))) {
+    // staging slots of the TMA path: barrier per slot
+    __shared__ uint64_t s_sbar[2];
+    constexpr int NJI = sizeof(PlaneJob) / sizeof(int), NPI = sizeof(FilterParams) / sizeof(int);
+    static_assert(NJI <= 64 && NPI <= 64 && NT >= 128, "descriptor size");
+    if (tid < NJI) reinterpret_cast<int*>(&s_job)[tid] = reinterpret_cast<const int*>(&a.jobs[lo])[tid];
+    if (tid >= 64 && tid < 64 + NPI) {
         const FilterParams* src = a.params ? a.params + a.jobs[lo].param : &a.p;
-        reinterpret_cast<int*>(&s_par)[tid - 32] = reinterpret_cast<const int*>(src)[tid - 32];
+        reinterpret_cast<int*>(&s_par)[tid - 64] = reinterpret_cast<const int*>(src)[tid - 64];
+    }
+    if (tid == 0) {
+        mbar_init(&s_sbar[0], 1);
+        mbar_init(&s_sbar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
     const PlaneJob& job = s_job;
@@ -863,34 +1067,99 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
     const int x0 = u.bx0 * S;            // footprint origin (padded coordinates)
     const int rowlen = nbx * S + O;      // footprint width
     const bool vec = ((S & 3) == 0);
+
+    // TMA staging: the S new rows of every frame of the next step are copied
+    // one row per box (row index through the mirror map, so no mirrored row
+    // needs a special path) into a staging slot while this step computes,
+    // then converted to FP32 into the input ring.  The box starts at xa, the
+    // footprint's first source column rounded down to 16 bytes (negative at
+    // the left edge: the copy fills zeros there, and the mirror map of the
+    // conversion never reads them).
+    const int esz_s = P.kind == kF32 ? 4 : (P.kind == kU16 ? 2 : 1);
+    const int al = 16 / esz_s;
+    const int xa = (x0 - ox) >= 0 ? ((x0 - ox) / al) * al : -(((ox - x0) + al - 1) / al) * al;
+    bool use_tma = a.tmaps != nullptr && job.tmap[0] >= 0;
+    {
+        // every source column the footprint reads, mirrored ones included, must lie in the box
+        const int c_lo = x0 - ox, c_hi = x0 - ox + rowlen - 1;
+        int need_lo = max(c_lo, 0), need_hi = min(c_hi, W - 1);
+        if (c_lo < 0) need_hi = max(need_hi, -c_lo);
+        if (c_hi >= W) need_lo = min(need_lo, 2 * (W - 1) - c_hi);
+        use_tma = use_tma && need_lo >= xa && need_hi < xa + a.stage_bw && need_lo >= 0 && need_hi < W;
+    }
+    const int srb = stage_row_bytes(a.stage_bw, esz_s);
+    // staging slots: the first 128-byte boundary at or after stage_off (the host adds 128 bytes)
+    unsigned char* s_stg = reinterpret_cast<unsigned char*>(sm) + a.stage_off;
+    s_stg += (128u - (smem_addr(s_stg) & 127u)) & 127u;
+    // Issued by the last warp (whose threads carry the fewest overlap-add
+    // items): lane 0 announces the bytes, then lane k copies row k % S of frame
+    // k / S of the next step (rows [n_lo_next, n_lo_next + S)) into slot
+    // j_next & 1.
+    auto tma_issue = [&](int j_next, int n_lo_next) {
+        const int slot = j_next & 1;
+        if (lane == 0) {
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(&s_sbar[slot], (uint32_t)(T * S * a.stage_bw * esz_s));
+        }
+        __syncwarp();
+        for (int k = lane; k < T * S; k += 32) {
+            const int t = k / S, r = k - t * S;
+            const unsigned char* map = reinterpret_cast<const unsigned char*>(a.tmaps) + (size_t)job.tmap[t] * kTmapBytes;
+            tma_load_2d(s_stg + ((slot * T + t) * S + r) * srb, map, xa, mirror(n_lo_next + r - oy, Hh),
+                        &s_sbar[slot]);
+        }
+    };
+    // Conversion items of the TMA path: (frame t, row r, chunk c of cw
+    // samples), the same every step; thread tid takes items NT - 1 - tid + j NT
+    // (the reverse order of the overlap-add items); the first CJ stay in
+    // registers.  Packed: t | r << 3 | c << 9 | fast << 17 (fast: four
+    // in-plane samples, aligned in the staged row).
+    const int cw = vec ? 4 : 1;
+    const int nch = rowlen / cw;
+    const int n_conv = use_tma ? T * S * nch : 0;
+    auto conv_item = [&](int ci) -> int {
+        const int t = ci / (S * nch);
+        const int rem = ci - t * S * nch;
+        const int r = rem / nch, c = rem - r * nch;
+        const int sc = x0 + c * cw - ox;
+        const int fast = (cw == 4 && sc >= 0 && sc + 4 <= W && ((sc - xa) & 3) == 0) ? 1 : 0;
+        return t | (r << 3) | (c << 9) | (fast << 17);
+    };
+    constexpr int CJ = 2;
+    int conv_it[CJ];
+#pragma unroll
+    for (int j = 0; j < CJ; ++j) conv_it[j] = NT - 1 - tid + j * NT < n_conv ? conv_item(NT - 1 - tid + j * NT) : -1;
     const int excl_y0 = u.by0 * S + O, excl_y1 = u.by1 * S;
     const int excl_x0 = x0 + O, excl_x1 = u.bx1 * S;
 
-    // input rows [r_lo, r_lo + nr) of every temporal plane: element i of the
-    // flattened (t, row, x) range -> (plane, ring offset, global index)
-    const int esz = P.kind == kF32 ? 4 : (P.kind == kU16 ? 2 : 1);
-    auto stage_item = [&](int i, int r_lo, int nr, float inv_nr_rl, float inv_rl, int& t, int& soff, long long& gidx) {
-        t = div_small(i, inv_nr_rl);
-        const int rem = i - t * nr * rowlen;
-        const int r = div_small(rem, inv_rl);
-        const int lx = rem - r * rowlen;
-        const int py = r_lo + r;
-        soff = (t * B + (py & (B - 1))) * pitch + lx;
-        gidx = (long long)mirror(py - oy, Hh) * job.src_stride + mirror(x0 + lx - ox, W);
-    };
     const float inv_rl = 1.0f / (float)rowlen;
     const float inv_S = 1.0f / (float)S;
+    const StageGeom sgeo{job.src, job.src_stride, P.kind, rowlen, pitch, x0, ox, oy, W, Hh};
     // prologue: the first B rows of the unit
-    {
-        const int nr = B;
-        const float inv_nr_rl = 1.0f / (float)(nr * rowlen);
-        for (int i = tid; i < T * nr * rowlen; i += NT) {
-            int t, soff;
-            long long gidx;
-            stage_item(i, u.by0 * S, nr, inv_nr_rl, inv_rl, t, soff, gidx);
-            s_in[soff] = load_sample(job.src[t], gidx, P.kind);
-        }
-    }
+    stage_rows_plain<B, T, NT>(s_in, sgeo, u.by0 * S, B, tid);
+
+    // Overlap-add items of the vector path (S a multiple of 4, so a segment
+    // of 4 pixels never straddles a block edge): item (r, q) is footprint row
+    // r of the step, pixels [4q, 4q + 4), covered by blocks b_lo .. b_lo +
+    // nk - 1; `ex` marks a segment inside the unit's exclusive columns and
+    // the plane.  Thread tid takes items tid + j NT; the first OJ stay in
+    // registers for the whole unit.  Packed: r | q << 5 | b_lo << 13 | nk <<
+    // 21 | ex << 25.
+    constexpr int OJ = 2;
+    const int nseg = rowlen >> 2;
+    const int n_ola = vec ? B * nseg : 0;
+    auto ola_item = [&](int i) -> int {
+        const int r = i / nseg, q = i - r * nseg;
+        const int px = 4 * q;
+        const int b_lo = px + 4 <= B ? 0 : (px + 4 - B + S - 1) / S;
+        const int b_hi = min(px / S, nbx - 1);
+        const int gx = x0 + px;
+        const int ex = (gx >= excl_x0 && gx + 4 <= excl_x1 && gx >= ox && gx + 4 <= ox + W) ? 1 : 0;
+        return r | (q << 5) | (b_lo << 13) | ((b_hi - b_lo + 1) << 21) | (ex << 25);
+    };
+    int ola_it[OJ];
+#pragma unroll
+    for (int j = 0; j < OJ; ++j) ola_it[j] = tid + j * NT < n_ola ? ola_item(tid + j * NT) : -1;
 
     // lane roles: rows (b, y) and columns (b, w = 2c + h), B lanes per block
     const int lb = lane / B, lw = lane % B;
@@ -898,10 +1167,11 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
     float* wbl = s_wbuf + bl * L::BSTR;
     const bool valid = bl < nbx;
     const int blr = valid ? bl : nbx - 1;
-    constexpr int PF = 4;  // input samples per thread carried in registers across the overlap-add
 
     for (int by = u.by0; by < u.by1; ++by) {
         __syncthreads();  // input rows of this step staged; block buffers free
+        // next step's new input rows: TMA copies in flight during this step
+        if (use_tma && warp == NW - 1 && by + 1 < u.by1) tma_issue(by + 1 - u.by0, by * S + B);
 
         // ---- per-warp block transforms (B lanes per block, BPW blocks per warp)
         {
@@ -919,24 +1189,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
         __syncthreads();  // block outputs complete; this step's input rows consumed
 
         const bool last = (by + 1 == u.by1);
-        // ---- next step's new input rows: loads issued now, stored after the overlap-add
-        const int n_lo = (by + 1) * S + B - S;
-        const int n_items = last ? 0 : T * S * rowlen;
-        const float inv_nr_rl = 1.0f / (float)(S * rowlen);
-        unsigned pf[PF];
-        int pf_off[PF];
-#pragma unroll
-        for (int k = 0; k < PF; ++k) {
-            const int i = tid + k * NT;
-            pf_off[k] = -1;
-            if (i < n_items) {
-                int t;
-                long long gidx;
-                stage_item(i, n_lo, S, inv_nr_rl, inv_rl, t, pf_off[k], gidx);
-                pf[k] = load_raw(job.src[t], gidx, P.kind);
-            }
-        }
-
+        const int n_lo = (by + 1) * S + B - S;  // first new input row of the next step
         // ---- overlap-add of this step's blocks into the ring; rows that no
         // later block reaches are final and leave the ring (same thread, no barrier)
         const int nfin = last ? B : S;
@@ -951,55 +1204,56 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
             }
         };
         if (vec) {
-            // items are pixel pairs (S, B multiples of 4: a pair never straddles a block edge)
-            const int nq = rowlen >> 1;
-            const float inv_nq = 1.0f / (float)nq;
-            for (int i = tid; i < B * nq; i += NT) {
-                const int r = div_small(i, inv_nq), q = i - r * nq;
-                const int px = 2 * q;
-                // blocks k with k*S <= px <= k*S + B - 2
-                const int b_lo = px <= B - 2 ? 0 : div_small(px - B + 1 + S, inv_S);
-                const int b_hi = min(div_small(px, inv_S), nbx - 1);
+            // segment items (see ola_item): ring cell + covering blocks in ascending order
+            auto do_item = [&](int it) {
+                const int r = it & 31, q = (it >> 5) & 255, b_lo = (it >> 13) & 255, nk = (it >> 21) & 15;
                 const int py = by * S + r;
-                float2* cell = reinterpret_cast<float2*>(s_ola + (py & (B - 1)) * pitch + px);
-                float2 acc = *cell;
-                if (B == 4 * S) {
-                    // at most four blocks: their loads are issued together, then
-                    // summed in ascending block order. Block k = b_hi - 3 + m
-                    // holds the pair at x = x_top + (3 - m) S, x_top = px - b_hi S;
-                    // S is a multiple of 4, so only the 4-float chunk index moves
-                    const int x_top = px - b_hi * S;
-                    const int off0 = (b_hi - 3) * L::BSTR + r * B + (x_top & 3);
-                    const int c0 = x_top >> 2, sw = TL::swz(r), sq = S >> 2;
-                    float2 v[4];
+                float4* cell = reinterpret_cast<float4*>(s_ola + (py & (B - 1)) * pitch + 4 * q);
+                float4 acc = *cell;
+                const int sw = TL::swz(r), sq = S >> 2;
+                const float* wb0 = s_wbuf + b_lo * L::BSTR + r * B;
+                const int c0 = q - b_lo * sq;  // 4-float chunk of segment q in block b_lo
+                constexpr int MK = B / 4 < 4 ? B / 4 : 4;  // loads issued together
+                float4 v[MK];
 #pragma unroll
-                    for (int m = 0; m < 4; ++m) {
-                        v[m] = b_hi - 3 + m >= b_lo
-                                   ? *reinterpret_cast<const float2*>(s_wbuf + off0 + m * L::BSTR +
-                                                                      (((c0 + (3 - m) * sq) ^ sw) << 2))
-                                   : make_float2(0.f, 0.f);
-                    }
+                for (int m = 0; m < MK; ++m)
+                    v[m] = m < nk ? *reinterpret_cast<const float4*>(wb0 + m * L::BSTR + (((c0 - m * sq) ^ sw) << 2))
+                                  : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-                    for (int m = 0; m < 4; ++m) {
-                        if (b_hi - 3 + m >= b_lo) {
-                            acc.x += v[m].x;
-                            acc.y += v[m].y;
-                        }
+                for (int m = 0; m < MK; ++m) {
+                    if (m < nk) {
+                        acc.x += v[m].x;
+                        acc.y += v[m].y;
+                        acc.z += v[m].z;
+                        acc.w += v[m].w;
                     }
-                } else {
-                    for (int k = b_lo; k <= b_hi; ++k) {
-                        const float2 v = *reinterpret_cast<const float2*>(s_wbuf + k * L::BSTR + TL::off(r, px - k * S));
-                        acc.x += v.x;
-                        acc.y += v.y;
-                    }
+                }
+                for (int m = MK; m < nk; ++m) {  // 32x32 blocks at block step 4
+                    const float4 w4 = *reinterpret_cast<const float4*>(wb0 + m * L::BSTR + (((c0 - m * sq) ^ sw) << 2));
+                    acc.x += w4.x;
+                    acc.y += w4.y;
+                    acc.z += w4.z;
+                    acc.w += w4.w;
                 }
                 if (r < nfin) {
-                    finish(py, px, acc.x);
-                    finish(py, px + 1, acc.y);
-                    acc = make_float2(0.f, 0.f);
+                    const int px = x0 + 4 * q;
+                    if (((it >> 25) & 1) && py >= excl_y0 && py < excl_y1 && py >= oy && py < oy + Hh) {
+                        store4(job.dst, (long long)(py - oy) * job.dst_stride + (px - ox), acc, P.kind, P.peak,
+                               inv_scale);
+                    } else {
+                        finish(py, 4 * q, acc.x);
+                        finish(py, 4 * q + 1, acc.y);
+                        finish(py, 4 * q + 2, acc.z);
+                        finish(py, 4 * q + 3, acc.w);
+                    }
+                    acc = make_float4(0.f, 0.f, 0.f, 0.f);
                 }
                 *cell = acc;
-            }
+            };
+#pragma unroll
+            for (int j = 0; j < OJ; ++j)
+                if (ola_it[j] >= 0) do_item(ola_it[j]);
+            for (int i = tid + OJ * NT; i < n_ola; i += NT) do_item(ola_item(i));
         } else {
             for (int i = tid; i < B * rowlen; i += NT) {
                 const int r = div_small(i, inv_rl), px = i - r * rowlen;
@@ -1018,31 +1272,37 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
             }
         }
 
-        // ---- store the prefetched rows (and any beyond the register budget)
-#pragma unroll
-        for (int k = 0; k < PF; ++k)
-            if (pf_off[k] >= 0) s_in[pf_off[k]] = raw_to_float(pf[k], P.kind);
-        for (int i = tid + PF * NT; i < n_items; i += NT) {
-            int t, soff;
-            long long gidx;
-            stage_item(i, n_lo, S, inv_nr_rl, inv_rl, t, soff, gidx);
-            s_in[soff] = load_sample(job.src[t], gidx, P.kind);
-        }
-        // warm L2 with the rows of the step after next (one request per 128 B)
-        if (by + 2 < u.by1) {
-            const int npy = n_lo + S;
-            const int sx_lo = max(x0 - ox, 0), sx_hi = max(min(x0 + rowlen - ox, W) - 1, sx_lo);
-            const int nline = (int)(((long long)(sx_hi - sx_lo) * esz) / 128) + 2;
-            for (int i = tid; i < T * S * nline; i += NT) {
-                const int t = i / (S * nline);
-                const int rem = i - t * S * nline;
-                const int r = rem / nline, li = rem - r * nline;
-                const int py = npy + r;
-                if (py >= ph) continue;
-                const long long sy_ = mirror(py - oy, Hh);
-                const int sxp = min(sx_lo + li * (128 / esz), sx_hi);
-                prefetch_l2(reinterpret_cast<const char*>(job.src[t]) + (sy_ * job.src_stride + sxp) * esz);
+        // ---- the next step's new input rows: by plain loads (planes the TMA copies cannot take)
+        if (!use_tma && !last) stage_rows_plain<B, T, NT>(s_in, sgeo, n_lo, S, tid);
+        // TMA path: wait for the next step's rows and convert them into the
+        // ring.  Items (t, r, 4-sample chunk) go to the threads from the top
+        // down, the reverse of the overlap-add items above (the first
+        // threads carry one overlap-add item more).
+        if (use_tma && !last) {
+            // step j's rows are the ((j - 1) / 2)-th use of slot j & 1 (step 0's come from the prologue)
+            const int j = by + 1 - u.by0, slot = j & 1;
+            const uint32_t parity = (uint32_t)(((j - 1) >> 1) & 1);
+            if (!mbar_wait(&s_sbar[slot], parity)) {
+                // the copies did not complete in time: record it, and let them land before
+                // this unit's shared memory can be handed to another unit
+                if (tid == 0) atomicExch(a.error_flag, 4);
+                mbar_wait(&s_sbar[slot], parity, 16 * kDefaultWaitLimit);
             }
+            auto do_conv = [&](int it) {
+                const int t = it & 7, r = (it >> 3) & 63, c = (it >> 9) & 255;
+                float* dst = s_in + (t * B + ((n_lo + r) & (B - 1))) * pitch + c * cw;
+                const unsigned char* srow = s_stg + ((slot * T + t) * S + r) * srb;
+                const int sc = x0 + c * cw - ox;  // source column of the first sample
+                if ((it >> 17) & 1) {
+                    *reinterpret_cast<float4*>(dst) = stage_load4(srow, sc - xa, P.kind);
+                } else {
+                    for (int i = 0; i < cw; ++i) dst[i] = stage_load1(srow, mirror(sc + i, W) - xa, P.kind);
+                }
+            };
+#pragma unroll
+            for (int jj = 0; jj < CJ; ++jj)
+                if (conv_it[jj] >= 0) do_conv(conv_it[jj]);
+            for (int ci = NT - 1 - tid + CJ * NT; ci < n_conv; ci += NT) do_conv(conv_item(ci));
         }
     }
 

@@ -59,11 +59,7 @@ struct TcArgs {
     int wait_limit;         // iteration limit of the in-loop waits for the tensor cores
 };
 
-// ---- PTX wrappers (tcgen05, mbarrier) --------------------------------------
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
+// ---- PTX wrappers (tcgen05) ------------------------------------------------
 // shared-memory matrix descriptor: K-major, no swizzle (8-row x 16-byte core
 // matrices; lbo = byte step between core matrices along K, sbo = along M/N)
 __device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
@@ -103,25 +99,6 @@ __device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t a, uint64_t b, uin
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                  :: "r"(smem_addr(bar)) : "memory");
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_addr(bar)), "r"(count) : "memory");
-}
-
-// bounded wait for the completion of the phase with the given parity; false
-// when `limit` polls ran out first
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int limit = kDefaultWaitLimit) {
-    const uint32_t a = smem_addr(bar);
-    for (int it = 0; it < limit; ++it) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done) : "r"(a), "r"(parity) : "memory");
-        if (done) return true;
-    }
-    return false;
 }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
