@@ -476,9 +476,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-peak", action="store_true", help="skip the SGEMM peak measurement (profiling runs)")
-    ap.add_argument("--workload", default="yuv1080p", choices=["yuv1080p", "batch", "batch_small"],
+    ap.add_argument("--workload", default="yuv1080p", choices=["yuv1080p", "batch", "batch_small", "autograd"],
                     help="batch: the 32-clip multi-clip batching workload (one GPU); batch_small: the same with "
-                         "640x360 clips only")
+                         "640x360 clips only; autograd: forward vs forward + backward of the differentiable path")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--fbf-frames", type=int, default=32,
                     help="frames filtered frame by frame through the cached per-plane host path (0 skips)")
@@ -489,6 +489,12 @@ def main():
     ap.add_argument("--extras", type=int, default=1,
                     help="0 skips the parity, differentiation and batching keys (profiling runs)")
     opts = ap.parse_args()
+    if opts.workload == "autograd":
+        if opts.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no gradient"}))
+            return
+        print(json.dumps(autograd_measure(opts.steps, opts.warmup)))
+        return
     if opts.workload in ("batch", "batch_small"):
         if opts.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no multi-clip batch"}))

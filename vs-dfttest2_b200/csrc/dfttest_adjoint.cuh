@@ -53,14 +53,14 @@ struct AdjointArgs {
     float* gsigma;         // [T][B][X], added to (may be null)
 };
 
-// m(psd, s) of frequency_filtering and its partial derivatives
-__device__ __forceinline__ void gain_grad(int ft, float psd, float s, const AdjointArgs& a, float& m, float& dpsd,
+// m(psd, s) of frequency_filtering and its partial derivatives, for filter type FT
+template <int FT>
+__device__ __forceinline__ void gain_grad(float psd, float s, const AdjointArgs& a, float& m, float& dpsd,
                                           float& dsig) {
     const float eps = 1e-15f;
     dpsd = 0.0f;
     dsig = 0.0f;
-    switch (ft) {
-    case 0: {
+    if constexpr (FT == 0) {
         const float den = psd + eps;
         const float u = (psd - s) / den;
         m = fmaxf(u, 0.0f);
@@ -68,22 +68,16 @@ __device__ __forceinline__ void gain_grad(int ft, float psd, float s, const Adjo
             dpsd = (s + eps) / (den * den);
             dsig = -1.0f / den;
         }
-        return;
-    }
-    case 1:
+    } else if constexpr (FT == 1) {
         m = psd < s ? 0.0f : 1.0f;
-        return;
-    case 2:
+    } else if constexpr (FT == 2) {
         m = s;
         dsig = 1.0f;
-        return;
-    case 3: {
+    } else if constexpr (FT == 3) {
         const bool in = psd >= a.pmin && psd <= a.pmax;
         m = in ? s : a.sigma2;
         dsig = in ? 1.0f : 0.0f;
-        return;
-    }
-    case 4: {
+    } else if constexpr (FT == 4) {
         const float D = (psd + a.pmin) * (psd + a.pmax) + eps;
         const float h = psd * a.pmax / D;
         const float sh = sqrtf(h);
@@ -93,23 +87,23 @@ __device__ __forceinline__ void gain_grad(int ft, float psd, float s, const Adjo
             const float dh = a.pmax / D - psd * a.pmax * (2.0f * psd + a.pmin + a.pmax) / (D * D);
             dpsd = s * dh / (2.0f * sh);
         }
-        return;
-    }
-    default: {  // 5: u^pmin, 6: sqrt(u)
+    } else {  // 5: u^pmin, 6: sqrt(u)
         const float den = psd + eps;
         const float u0 = (psd - s) / den;
         const float u = fmaxf(u0, 0.0f);
-        const float p = ft == 5 ? a.pmin : 0.5f;
-        m = ft == 5 ? powf(u, p) : sqrtf(u);
+        const float p = FT == 5 ? a.pmin : 0.5f;
+        m = FT == 5 ? powf(u, p) : sqrtf(u);
         if (u0 > 0.0f) {
             const float dmu = p * m / u;
             dpsd = dmu * (s + eps) / (den * den);
             dsig = -dmu / den;
         }
-        return;
-    }
     }
 }
+
+template <int V> struct IntC {
+    static constexpr int value = V;
+};
 
 template <int B> __device__ __forceinline__ void r2c_n(const float (&x)[B], float (&y)[B]) {
     if constexpr (B == 8) r2c_8(x, y);
@@ -346,26 +340,39 @@ __global__ void __launch_bounds__(256) dfttest_adjoint_kernel(const __grid_const
             const float* ci = gi + gblk * B * X;
             const float g = a.zero_mean ? br[0] / wf0 : 0.0f;
             float dg = 0.0f;
+            // the filter type is uniform: one switch around the bins keeps the executed code one straight run
+            auto bins = [&](auto ftc) {
+                constexpr int FT = decltype(ftc)::value;
 #pragma unroll
-            for (int k = 0; k < L::NPER; ++k) {
-                const int i = gj + k * GT;
-                if (SPEC % GT == 0 || i < SPEC) {
-                    const int kt = i / (B * X), bin = i - kt * (B * X);
-                    const float cs = s_tw[2 * kt], sn = s_tw[2 * kt + 1];
-                    const float Gr = cr[bin] * cs - ci[bin] * sn;
-                    const float Gi = cr[bin] * sn + ci[bin] * cs;
-                    const float wr = s_wf[2 * i], wi = s_wf[2 * i + 1];
-                    const float dr = br[i] - g * wr, di = bi[i] - g * wi;
-                    float m, dpsd, dsig;
-                    gain_grad(a.filter_type, dr * dr + di * di, s_sig[i], a, m, dpsd, dsig);
-                    const float q = Gr * dr + Gi * di;
-                    const float ddr = m * Gr + 2.0f * dpsd * q * dr;
-                    const float ddi = m * Gi + 2.0f * dpsd * q * di;
-                    acc[k] += dsig * q;
-                    dg += (Gr * wr + Gi * wi) - (ddr * wr + ddi * wi);
-                    br[i] = ddr;
-                    bi[i] = ddi;
+                for (int k = 0; k < L::NPER; ++k) {
+                    const int i = gj + k * GT;
+                    if (SPEC % GT == 0 || i < SPEC) {
+                        const int kt = i / (B * X), bin = i - kt * (B * X);
+                        const float cs = s_tw[2 * kt], sn = s_tw[2 * kt + 1];
+                        const float Gr = cr[bin] * cs - ci[bin] * sn;
+                        const float Gi = cr[bin] * sn + ci[bin] * cs;
+                        const float wr = s_wf[2 * i], wi = s_wf[2 * i + 1];
+                        const float dr = br[i] - g * wr, di = bi[i] - g * wi;
+                        float m, dpsd, dsig;
+                        gain_grad<FT>(dr * dr + di * di, s_sig[i], a, m, dpsd, dsig);
+                        const float q = Gr * dr + Gi * di;
+                        const float ddr = m * Gr + 2.0f * dpsd * q * dr;
+                        const float ddi = m * Gi + 2.0f * dpsd * q * di;
+                        acc[k] += dsig * q;
+                        dg += (Gr * wr + Gi * wi) - (ddr * wr + ddi * wi);
+                        br[i] = ddr;
+                        bi[i] = ddi;
+                    }
                 }
+            };
+            switch (a.filter_type) {
+            case 0: bins(IntC<0>{}); break;
+            case 1: bins(IntC<1>{}); break;
+            case 2: bins(IntC<2>{}); break;
+            case 3: bins(IntC<3>{}); break;
+            case 4: bins(IntC<4>{}); break;
+            case 5: bins(IntC<5>{}); break;
+            default: bins(IntC<6>{}); break;
             }
             constexpr int RW = GT < 32 ? GT : 32;
 #pragma unroll
