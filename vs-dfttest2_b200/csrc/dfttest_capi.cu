@@ -719,10 +719,15 @@ int launch(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, floa
     a.error_flag = slot.d_error;
     // full-height strips: the unit kernel sums its seams itself
     const bool inline_seams = plan.nfix > 0 && plan.full_strips && plan.nseams > 0;
-    if (inline_seams) {
-        if (int rc = ensure(slot.d_seams, slot.seams_cap, (size_t)plan.nseams, slot.done)) return rc;
-        CUDA_TRY(cudaMemsetAsync(slot.d_seams, 0, (size_t)plan.nseams * sizeof(int), stream));
-        a.seam_count = slot.d_seams;
+    // persistent grid (a work counter after the seam counters; both zeroed by one memset)
+    const char* penv = std::getenv("DFTTEST2_B200_PERSISTENT");
+    const bool persistent = !(penv && std::atoi(penv) == 0);
+    if (inline_seams || persistent) {
+        const size_t ncount = (size_t)(inline_seams ? plan.nseams : 0) + 1;
+        if (int rc = ensure(slot.d_seams, slot.seams_cap, ncount, slot.done)) return rc;
+        CUDA_TRY(cudaMemsetAsync(slot.d_seams, 0, ncount * sizeof(int), stream));
+        if (inline_seams) a.seam_count = slot.d_seams;
+        if (persistent) a.unit_counter = slot.d_seams + (inline_seams ? plan.nseams : 0);
     }
 
     if (bw > 0) {
@@ -732,7 +737,13 @@ int launch(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, floa
     }
     KernelFn kern = (f->filter_type == 0 && !f->asym && !sig_override) ? f->var.main : f->var.generic;
     CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<plan.nunits, f->var.nw * 32, smem, stream>>>(a);
+    int grid = plan.nunits;
+    if (persistent) {  // one CTA per resident slot
+        int per_sm = 0;
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, f->var.nw * 32, smem));
+        grid = std::min(plan.nunits, std::max(1, per_sm) * f->num_sms);
+    }
+    kern<<<grid, f->var.nw * 32, smem, stream>>>(a);
     CUDA_TRY(cudaGetLastError());
     if (plan.nfix > 0 && !inline_seams) {
         const int threads = 256;

@@ -147,6 +147,10 @@ struct KernelArgs {
     const void* tmaps;
     int stage_bw;
     int stage_off;
+    // Persistent grid: after its first unit (blockIdx.x) a CTA takes unit
+    // gridDim.x + atomicAdd(unit_counter, 1) until none is left; the counter
+    // is zeroed before the launch.  Null: one unit per CTA.
+    int* unit_counter;
 };
 
 constexpr int kTmapBytes = 128;
@@ -991,29 +995,34 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
     const int pitch = a.ring_pitch;
 
     // --- locate the unit ---------------------------------------------------
-    const int uid = blockIdx.x;
-    int lo = 0, hi = a.njobs - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (a.jobs[mid].unit_base <= uid) lo = mid; else hi = mid - 1;
-    }
     // the plane descriptor is read many times per step: keep it on chip
     __shared__ PlaneJob s_job;
     // and so are its format and filter
     __shared__ FilterParams s_par;
     // staging slots of the TMA path: barrier per slot
     __shared__ uint64_t s_sbar[2];
+    __shared__ int s_next;
     constexpr int NJI = sizeof(PlaneJob) / sizeof(int), NPI = sizeof(FilterParams) / sizeof(int);
     static_assert(NJI <= 64 && NPI <= 64 && NT >= 128, "descriptor size");
-    if (tid < NJI) reinterpret_cast<int*>(&s_job)[tid] = reinterpret_cast<const int*>(&a.jobs[lo])[tid];
-    if (tid >= 64 && tid < 64 + NPI) {
-        const FilterParams* src = a.params ? a.params + a.jobs[lo].param : &a.p;
-        reinterpret_cast<int*>(&s_par)[tid - 64] = reinterpret_cast<const int*>(src)[tid - 64];
-    }
     if (tid == 0) {
         mbar_init(&s_sbar[0], 1);
         mbar_init(&s_sbar[1], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // TMA batches this CTA has issued: batch n uses slot n & 1, and is that
+    // slot's (n >> 1)-th phase
+    uint32_t tma_batches = 0;
+
+    for (int uid = blockIdx.x; uid < a.nunits;) {
+    int lo = 0, hi = a.njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (a.jobs[mid].unit_base <= uid) lo = mid; else hi = mid - 1;
+    }
+    if (tid < NJI) reinterpret_cast<int*>(&s_job)[tid] = reinterpret_cast<const int*>(&a.jobs[lo])[tid];
+    if (tid >= 64 && tid < 64 + NPI) {
+        const FilterParams* src = a.params ? a.params + a.jobs[lo].param : &a.p;
+        reinterpret_cast<int*>(&s_par)[tid - 64] = reinterpret_cast<const int*>(src)[tid - 64];
     }
     __syncthreads();
     const PlaneJob& job = s_job;
@@ -1026,7 +1035,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
     const int sx = lid % job.nsx, sy = lid / job.nsx;
     const UnitGeom u = unit_geom(sx, sy, job.nsx, job.nsy, pnx, pny, B, S);
     const int nbx = u.bx1 - u.bx0;
-    if (nbx > BPS) {
+    if (nbx > BPS) {  // uniform: no thread of the CTA touches this unit
         if (tid == 0) atomicExch(a.error_flag, 1);
         return;
     }
@@ -1095,8 +1104,8 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
     // items): lane 0 announces the bytes, then lane k copies row k % S of frame
     // k / S of the next step (rows [n_lo_next, n_lo_next + S)) into slot
     // j_next & 1.
-    auto tma_issue = [&](int j_next, int n_lo_next) {
-        const int slot = j_next & 1;
+    auto tma_issue = [&](uint32_t batch, int n_lo_next) {
+        const int slot = batch & 1;
         if (lane == 0) {
             fence_proxy_async_smem();
             mbar_arrive_expect_tx(&s_sbar[slot], (uint32_t)(T * S * a.stage_bw * esz_s));
@@ -1171,7 +1180,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
     for (int by = u.by0; by < u.by1; ++by) {
         __syncthreads();  // input rows of this step staged; block buffers free
         // next step's new input rows: TMA copies in flight during this step
-        if (use_tma && warp == NW - 1 && by + 1 < u.by1) tma_issue(by + 1 - u.by0, by * S + B);
+        if (use_tma && warp == NW - 1 && by + 1 < u.by1) tma_issue(tma_batches, by * S + B);
 
         // ---- per-warp block transforms (B lanes per block, BPW blocks per warp)
         {
@@ -1279,9 +1288,10 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
         // down, the reverse of the overlap-add items above (the first
         // threads carry one overlap-add item more).
         if (use_tma && !last) {
-            // step j's rows are the ((j - 1) / 2)-th use of slot j & 1 (step 0's come from the prologue)
-            const int j = by + 1 - u.by0, slot = j & 1;
-            const uint32_t parity = (uint32_t)(((j - 1) >> 1) & 1);
+            // the batch issued at the top of this step
+            const int slot = tma_batches & 1;
+            const uint32_t parity = (tma_batches >> 1) & 1;
+            ++tma_batches;
             if (!mbar_wait(&s_sbar[slot], parity)) {
                 // the copies did not complete in time: record it, and let them land before
                 // this unit's shared memory can be handed to another unit
@@ -1338,6 +1348,14 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
                              is_float ? 0.0f : inv_scale);
             }
         }
+    }
+
+    // ---- the next unit (persistent grid)
+    if (a.unit_counter == nullptr) break;
+    __syncthreads();  // this unit's work is done before its descriptor and rings are replaced
+    if (tid == 0) s_next = (int)gridDim.x + atomicAdd(a.unit_counter, 1);
+    __syncthreads();
+    uid = s_next;
     }
 }
 
