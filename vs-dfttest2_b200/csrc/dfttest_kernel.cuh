@@ -49,6 +49,22 @@ enum SampleKind : int { kU8 = 0, kU16 = 1, kF32 = 2 };
 // polls of a bounded device wait before it gives up and reports an error
 constexpr int kDefaultWaitLimit = 1 << 22;
 
+// Checked build (-DDFT_CHECKS): the unit and fix-up kernels test their
+// shared-memory ring, staging and block-buffer indices and their global
+// band-record, source and output indices against the buffers before each
+// access; an index outside its buffer skips the access and records error
+// code 3 (nothing traps).  The normal build compiles the tests away.
+#ifdef DFT_CHECKS
+__device__ __forceinline__ bool in_range(long long i, long long n, int* flag) {
+    if (i >= 0 && i < n) return true;
+    atomicExch(flag, 3);
+    return false;
+}
+#define DFT_IN_RANGE(i, n, flag) ::dft2::in_range((long long)(i), (long long)(n), (flag))
+#else
+#define DFT_IN_RANGE(i, n, flag) true
+#endif
+
 // ---- PTX wrappers: shared-memory mbarriers and TMA tile loads ---------------
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -957,6 +973,7 @@ struct StageGeom {
     const void* const* src;  // the job's 2r+1 source planes
     long long src_stride;
     int kind, rowlen, pitch, x0, ox, oy, W, H;
+    int* err;                // error word (checked build)
 };
 template <int B, int T, int NT>
 __device__ __noinline__ void stage_rows_plain(float* __restrict__ s_in, const StageGeom g, int r_lo, int nr, int tid) {
@@ -968,8 +985,12 @@ __device__ __noinline__ void stage_rows_plain(float* __restrict__ s_in, const St
         const int r = div_small(rem, inv_rl);
         const int lx = rem - r * g.rowlen;
         const int py = r_lo + r;
-        const long long gidx = (long long)mirror(py - g.oy, g.H) * g.src_stride + mirror(g.x0 + lx - g.ox, g.W);
-        s_in[(t * B + (py & (B - 1))) * g.pitch + lx] = load_sample(g.src[t], gidx, g.kind);
+        const int sy = mirror(py - g.oy, g.H), sx = mirror(g.x0 + lx - g.ox, g.W);
+        const long long gidx = (long long)sy * g.src_stride + sx;
+        const int si = (t * B + (py & (B - 1))) * g.pitch + lx;
+        if (DFT_IN_RANGE(sy, g.H, g.err) && DFT_IN_RANGE(sx, g.W, g.err) && DFT_IN_RANGE(lx, g.pitch, g.err) &&
+            DFT_IN_RANGE(si, T * B * g.pitch, g.err))
+            s_in[si] = load_sample(g.src[t], gidx, g.kind);
     }
 }
 
@@ -1143,7 +1164,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
 
     const float inv_rl = 1.0f / (float)rowlen;
     const float inv_S = 1.0f / (float)S;
-    const StageGeom sgeo{job.src, job.src_stride, P.kind, rowlen, pitch, x0, ox, oy, W, Hh};
+    const StageGeom sgeo{job.src, job.src_stride, P.kind, rowlen, pitch, x0, ox, oy, W, Hh, a.error_flag};
     // prologue: the first B rows of the unit
     stage_rows_plain<B, T, NT>(s_in, sgeo, u.by0 * S, B, tid);
 
@@ -1185,8 +1206,9 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
         // ---- per-warp block transforms (B lanes per block, BPW blocks per warp)
         {
             // row phase: the DC of each block is summed over its rows with shuffles
-            const float dc =
-                row_task<B, T>(wbl, s_in, pitch, (by * S + lw) & (B - 1), blr * S, t_win, P.scale, lw, vec, valid);
+            int xoff = blr * S;
+            if (!DFT_IN_RANGE(xoff + B - 1, pitch, a.error_flag)) xoff = 0;
+            const float dc = row_task<B, T>(wbl, s_in, pitch, (by * S + lw) & (B - 1), xoff, t_win, P.scale, lw, vec, valid);
             const float tot = block_row_sum<B>(dc);
             // g = DC / Re(WF[0]) (cpu_source/kernel.hpp:1945)
             if (lw == 0 && valid) s_g[bl] = P.g_div != 0.0f ? __fdiv_rn(tot, P.g_div) : 0.0f;
@@ -1209,7 +1231,8 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
                 store_sample(job.dst, (long long)(py - oy) * job.dst_stride + (px - ox), v, P.kind, P.scale, P.peak,
                              is_float ? 0.0f : inv_scale);
             } else {
-                rec[band_index(lx, py - u.by0 * S, fw, u.fh, O)] = v;
+                const int bi = band_index(lx, py - u.by0 * S, fw, u.fh, O);
+                if (DFT_IN_RANGE(bi, a.rec_stride, a.error_flag)) rec[bi] = v;
             }
         };
         if (vec) {
@@ -1217,6 +1240,13 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
             auto do_item = [&](int it) {
                 const int r = it & 31, q = (it >> 5) & 255, b_lo = (it >> 13) & 255, nk = (it >> 21) & 15;
                 const int py = by * S + r;
+#ifdef DFT_CHECKS
+                if (!DFT_IN_RANGE((py & (B - 1)) * pitch + 4 * q + 3, L::ola_floats(pitch), a.error_flag) ||
+                    !DFT_IN_RANGE(4 * q + 3, pitch, a.error_flag) || !DFT_IN_RANGE(b_lo + nk - 1, nbx, a.error_flag))
+                    return;
+                for (int m = 0; m < nk; ++m)
+                    if (!DFT_IN_RANGE(q - (b_lo + m) * (S >> 2), B / 4, a.error_flag)) return;
+#endif
                 float4* cell = reinterpret_cast<float4*>(s_ola + (py & (B - 1)) * pitch + 4 * q);
                 float4 acc = *cell;
                 const int sw = TL::swz(r), sq = S >> 2;
@@ -1246,7 +1276,8 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
                 }
                 if (r < nfin) {
                     const int px = x0 + 4 * q;
-                    if (((it >> 25) & 1) && py >= excl_y0 && py < excl_y1 && py >= oy && py < oy + Hh) {
+                    if (((it >> 25) & 1) && py >= excl_y0 && py < excl_y1 && py >= oy && py < oy + Hh &&
+                        DFT_IN_RANGE(px - ox + 3, W, a.error_flag)) {
                         store4(job.dst, (long long)(py - oy) * job.dst_stride + (px - ox), acc, P.kind, P.peak,
                                inv_scale);
                     } else {
@@ -1303,6 +1334,14 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
                 float* dst = s_in + (t * B + ((n_lo + r) & (B - 1))) * pitch + c * cw;
                 const unsigned char* srow = s_stg + ((slot * T + t) * S + r) * srb;
                 const int sc = x0 + c * cw - ox;  // source column of the first sample
+#ifdef DFT_CHECKS
+                if (!DFT_IN_RANGE((t * B + ((n_lo + r) & (B - 1))) * pitch + c * cw + cw - 1, T * B * pitch,
+                                  a.error_flag) ||
+                    !DFT_IN_RANGE(((slot * T + t) * S + r) * srb, stage_bytes(a.stage_bw, esz_s, T, S), a.error_flag))
+                    return;
+                for (int i = 0; i < cw; ++i)
+                    if (!DFT_IN_RANGE(mirror(sc + i, W) - xa, a.stage_bw, a.error_flag)) return;
+#endif
                 if ((it >> 17) & 1) {
                     *reinterpret_cast<float4*>(dst) = stage_load4(srow, sc - xa, P.kind);
                 } else {
@@ -1342,8 +1381,11 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
                 const int r = i / O;
                 const int py = oy + r, px = pxs + (i - r * O);
                 if (px < ox || px >= ox + W) continue;
-                const float v = 0.0f + __ldcg(recl + band_index(px - ul.bx0 * S, py - ul.by0 * S, ul.fw, ul.fh, O)) +
-                                __ldcg(recr + band_index(px - ur.bx0 * S, py - ur.by0 * S, ur.fw, ur.fh, O));
+                const int il = band_index(px - ul.bx0 * S, py - ul.by0 * S, ul.fw, ul.fh, O);
+                const int ir = band_index(px - ur.bx0 * S, py - ur.by0 * S, ur.fw, ur.fh, O);
+                if (!DFT_IN_RANGE(il, a.rec_stride, a.error_flag) || !DFT_IN_RANGE(ir, a.rec_stride, a.error_flag))
+                    continue;
+                const float v = 0.0f + __ldcg(recl + il) + __ldcg(recr + ir);
                 store_sample(job.dst, (long long)(py - oy) * job.dst_stride + (px - ox), v, P.kind, P.scale, P.peak,
                              is_float ? 0.0f : inv_scale);
             }
@@ -1417,7 +1459,9 @@ __global__ void __launch_bounds__(256) dfttest_fixup_kernel(const __grid_constan
             for (int sx = sxl; sx <= sxh; ++sx) {
                 const UnitGeom u = unit_geom(sx, sy, job.nsx, job.nsy, pnx, pny, B, S);
                 const int uid = job.unit_base + sy * job.nsx + sx;
-                acc += a.scratch[(size_t)uid * a.rec_stride + band_index(px - u.bx0 * S, py - u.by0 * S, u.fw, u.fh, O)];
+                const int bi = band_index(px - u.bx0 * S, py - u.by0 * S, u.fw, u.fh, O);
+                if (DFT_IN_RANGE(bi, a.rec_stride, a.error_flag) && DFT_IN_RANGE(uid, a.nunits, a.error_flag))
+                    acc += a.scratch[(size_t)uid * a.rec_stride + bi];
             }
         }
         store_sample(job.dst, (long long)(py - oy) * job.dst_stride + (px - ox), acc, P.kind, P.scale, P.peak);

@@ -11,7 +11,10 @@ import os
 from ctypes import POINTER, c_char_p, c_double, c_int, c_ssize_t, c_void_p
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libdfttest2_b200.so")
+# DFTTEST2_B200_LIB=checked loads the bounds-checked build (make checked),
+# whose kernels record out-of-range indices as kernel error 3
+LIB_PATH = os.path.join(_HERE, "libdfttest2_b200_checked.so" if os.environ.get("DFTTEST2_B200_LIB") == "checked"
+                        else "libdfttest2_b200.so")
 
 NOALLOC_SCRATCH_BYTES = 8 * 1024 * 1024
 OK = 0
