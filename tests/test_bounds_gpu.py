@@ -57,7 +57,8 @@ def _run_guarded(flt, clip, st, bits, aligned, torch):
     src = torch.from_numpy(clip.view(np.uint8).reshape(n, h, w * esz)).cuda()
     src_strided = torch.zeros((n, h, stride), dtype=torch.uint8, device="cuda")
     src_strided[:, :, xoff * esz:xoff * esz + w * esz] = src
-    dst = torch.full((n, rows, stride + esz), CANARY, dtype=torch.uint8, device="cuda")
+    frame_bytes = rows * stride + 64  # 64 guard bytes after the last guard row
+    dst = torch.full((n, frame_bytes), CANARY, dtype=torch.uint8, device="cuda")
     r = flt.radius
     planes = []
     for i in range(n):
@@ -68,12 +69,13 @@ def _run_guarded(flt, clip, st, bits, aligned, torch):
     flt.check()
     d = dst.cpu().numpy()
     inside = np.zeros(d.shape, bool)
+    starts = []
     for y in range(h):
-        row = GUARD_ROWS + y
-        inside[:, row, xoff * esz:xoff * esz + w * esz] = True
+        s0 = (GUARD_ROWS + y) * stride + xoff * esz
+        inside[:, s0:s0 + w * esz] = True
+        starts.append(s0)
     intact = bool(np.all(d[~inside] == CANARY))
-    out = np.stack([d[i, GUARD_ROWS:GUARD_ROWS + h, xoff * esz:xoff * esz + w * esz].copy().view(clip.dtype)
-                    for i in range(n)])
+    out = np.stack([np.stack([d[i, s0:s0 + w * esz] for s0 in starts]).view(clip.dtype) for i in range(n)])
     return out, intact
 
 
