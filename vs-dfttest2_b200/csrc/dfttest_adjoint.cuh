@@ -156,11 +156,16 @@ template <int B, int T>
 struct AdjTile {
     static constexpr int X = B / 2 + 1;
     static constexpr int SPEC = T * B * X;  // complex bins of a block
+    // 8x8 and 16x16 blocks with up to 3 frames: tiles of 4 x 3 blocks on 12
+    // warps (two CTAs per SM at up to 85 registers); longer temporal sizes
+    // and 32x32 blocks need more registers per thread and run 8 warps
+    static constexpr bool WIDE = B <= 16 && T <= 3;
     static constexpr int TBX = B == 32 ? 2 : 4;
-    static constexpr int TBY = B == 32 ? (T >= 5 ? 1 : 2) : (B == 16 && T >= 5 ? 2 : 4);
+    static constexpr int TBY = WIDE ? 3 : (B == 32 ? (T >= 5 ? 1 : 2) : (B == 16 && T >= 5 ? 2 : 4));
     static constexpr int NBLK = TBX * TBY;
-    static constexpr int NTH = 256;
+    static constexpr int NTH = WIDE ? 384 : 256;
     static constexpr int GT = NTH / NBLK;              // threads per block in the gain phase
+    static_assert(NTH % NBLK == 0 && (GT & (GT - 1)) == 0, "the zero-mean reduction shuffles over a power of two");
     static constexpr int NPER = (SPEC + GT - 1) / GT;  // gain bins per thread
     // shared memory (floats), in order
     static constexpr int o_win = 0;                    // scale * window   [T][B][B]
@@ -169,12 +174,22 @@ struct AdjTile {
     static constexpr int o_wf = o_sig + SPEC;          // window spectrum  [SPEC][2]
     static constexpr int o_tw = o_wf + 2 * SPEC;       // conj temporal twiddles [T][2]
     static constexpr int o_dg = o_tw + 2 * T;          // zero-mean partials [NBLK]
-    static constexpr int o_zr = (o_dg + NBLK + 3) & ~3;  // spectra [NBLK][SPEC]
-    static constexpr int o_zi = o_zr + NBLK * SPEC;
-    static constexpr int o_gr = o_zi + NBLK * SPEC;    // output-gradient spectra [NBLK][B][X]
+    static constexpr int o_gs = o_dg + NBLK;           // sigma-gradient partials of the CTA [SPEC]
+    // spectra [NBLK][T][B][X]: temporal planes TS floats apart, TS = X (mod
+    // 32), so that the X-bin runs of the T planes that the column passes read
+    // side by side fall in disjoint shared-memory banks
+    static constexpr int TS = B * X + (((X - B * X) % 32) + 32) % 32;
+    static constexpr int ZB = T * TS;                  // floats per block
+    static constexpr int o_zr = (o_gs + SPEC + 3) & ~3;  // spectra [NBLK][ZB]
+    static constexpr int o_zi = o_zr + NBLK * ZB;
+    static constexpr int o_gr = o_zi + NBLK * ZB;      // output-gradient spectra [NBLK][B][X]
     static constexpr int o_gi = o_gr + NBLK * B * X;
-    static constexpr int o_dx = o_gi + NBLK * B * X;   // source-gradient patch [T][patch_h][patch_w]
-    static size_t smem_bytes(int ph, int pw) { return sizeof(float) * ((size_t)o_dx + (size_t)T * ph * pw); }
+    static constexpr int o_dx = o_gi + NBLK * B * X;   // the tile's source patch, then its gradient [T][patch_h][pitch]
+    // patch rows are an odd number of floats apart (bank spread of the row tasks)
+    __host__ __device__ static int patch_pitch(int pw) { return pw | 1; }
+    static size_t smem_bytes(int ph, int pw) {
+        return sizeof(float) * ((size_t)o_dx + (size_t)T * ph * patch_pitch(pw));
+    }
 };
 
 // rows of a packed real-spectrum layout <-> complex (kx = 0..B/2) arrays
@@ -192,9 +207,10 @@ __device__ __forceinline__ void packed_to_complex(const float (&y)[B], float* re
 }
 
 template <int B, int T>
-__global__ void __launch_bounds__(256) dfttest_adjoint_kernel(const __grid_constant__ AdjointArgs a) {
+__global__ void __launch_bounds__(AdjTile<B, T>::NTH, 2) dfttest_adjoint_kernel(const __grid_constant__ AdjointArgs a) {
     using L = AdjTile<B, T>;
     constexpr int X = L::X, SPEC = L::SPEC, NBLK = L::NBLK, TBX = L::TBX, TBY = L::TBY, GT = L::GT;
+    constexpr int TS = L::TS, ZB = L::ZB;
     constexpr int R = (T - 1) / 2;
     extern __shared__ __align__(16) float smem[];
     float* s_win = smem + L::o_win;
@@ -209,8 +225,7 @@ __global__ void __launch_bounds__(256) dfttest_adjoint_kernel(const __grid_const
     float* gi = smem + L::o_gi;
     float* dxp = smem + L::o_dx;
     const int tid = threadIdx.x;
-    const int S = a.block_step, PH = a.patch_h, PW = a.patch_w;
-    const int npatch = T * PH * PW;
+    const int S = a.block_step, PH = a.patch_h, PW = a.patch_w, PP = L::patch_pitch(a.patch_w);
 
     for (int i = tid; i < T * B * B; i += L::NTH) s_win[i] = a.scale * a.win[i];
     for (int i = tid; i < B * B; i += L::NTH) s_wsyn[i] = a.wsyn[i] / a.scale;
@@ -225,13 +240,13 @@ __global__ void __launch_bounds__(256) dfttest_adjoint_kernel(const __grid_const
         s_tw[2 * tid] = cs;
         s_tw[2 * tid + 1] = sn;
     }
-    for (int i = tid; i < npatch; i += L::NTH) dxp[i] = 0.0f;
     const float wf0 = a.zero_mean ? a.wf[0] : 1.0f;
     // gain-phase ownership: block gblk of the tile, bins gj + k GT
     const int gblk = tid / GT, gj = tid - gblk * GT;
-    float acc[L::NPER];
-#pragma unroll
-    for (int k = 0; k < L::NPER; ++k) acc[k] = 0.0f;
+    // sigma-gradient partials of the CTA (summed over its tiles in shared
+    // memory rather than registers, which leaves room for a third CTA per SM)
+    float* s_gs = smem + L::o_gs;
+    for (int i = tid; i < SPEC; i += L::NTH) s_gs[i] = 0.0f;
 
     for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
         int lo = 0, hi = a.njobs - 1;
@@ -248,7 +263,19 @@ __global__ void __launch_bounds__(256) dfttest_adjoint_kernel(const __grid_const
         const int ty = lt / job.ntx, tx = lt - ty * job.ntx;
         const int bx0 = tx * TBX, by0 = ty * TBY;
         if (tid < NBLK) s_dg[tid] = 0.0f;
-        __syncthreads();  // tables, patch zeroing and the previous tile's flush are complete
+        const int py0 = by0 * S, px0 = bx0 * S;
+        __syncthreads();  // tables and the previous tile's flush are complete
+        // the tile's source patch (T frames, PH x PW samples through the mirror), coalesced
+        for (int i = tid; i < T * PH * PW; i += L::NTH) {
+            const int t = i / (PH * PW), rem = i - t * (PH * PW);
+            const int r = rem / PW, c = rem - r * PW;
+            const int py = py0 + r, px = px0 + c;
+            dxp[(t * PH + r) * PP + c] =
+                (py < ph && px < pw)
+                    ? __ldg(job.src[t] + (long long)mirror(py - oy, Hh) * job.src_stride + mirror(px - ox, W))
+                    : 0.0f;
+        }
+        __syncthreads();
 
         // ---- rows: r2c_x of the windowed source blocks (t < T) and of the
         //      weighted output gradient (t == T, bins 0 < kx < B/2 doubled)
@@ -261,15 +288,15 @@ __global__ void __launch_bounds__(256) dfttest_adjoint_kernel(const __grid_const
             float v[B], o[B];
             if (t < T) {
                 if (valid) {
-                    const float* row = job.src[t] + (long long)mirror(py - oy, Hh) * job.src_stride;
+                    const float* row = dxp + (t * PH + (blk / TBX) * S + y) * PP + (blk % TBX) * S;
 #pragma unroll
-                    for (int x = 0; x < B; ++x) v[x] = s_win[(t * B + y) * B + x] * __ldg(row + mirror(px0 + x - ox, W));
+                    for (int x = 0; x < B; ++x) v[x] = s_win[(t * B + y) * B + x] * row[x];
                 } else {
 #pragma unroll
                     for (int x = 0; x < B; ++x) v[x] = 0.0f;
                 }
                 r2c_n<B>(v, o);
-                packed_to_complex<B>(o, zr + blk * SPEC + (t * B + y) * X, zi + blk * SPEC + (t * B + y) * X);
+                packed_to_complex<B>(o, zr + blk * ZB + t * TS + y * X, zi + blk * ZB + t * TS + y * X);
             } else {
                 const bool rin = valid && py >= oy && py < oy + Hh;
                 const float* row = job.gdst + (long long)(rin ? py - oy : 0) * job.gdst_stride;
@@ -290,13 +317,15 @@ __global__ void __launch_bounds__(256) dfttest_adjoint_kernel(const __grid_const
             }
         }
         __syncthreads();
+        // the patch now accumulates the source gradient (used again after the inverse transforms)
+        for (int i = tid; i < T * PH * PP; i += L::NTH) dxp[i] = 0.0f;
 
         // ---- columns: DFT_y of every (t, kx) column and of the gradient columns
         for (int task = tid; task < NBLK * (T + 1) * X; task += L::NTH) {
             const int blk = task / ((T + 1) * X), rem = task - blk * ((T + 1) * X);
             const int t = rem / X, kx = rem - t * X;
-            float* pr = t < T ? zr + blk * SPEC + t * B * X + kx : gr + blk * B * X + kx;
-            float* pi = t < T ? zi + blk * SPEC + t * B * X + kx : gi + blk * B * X + kx;
+            float* pr = t < T ? zr + blk * ZB + t * TS + kx : gr + blk * B * X + kx;
+            float* pi = t < T ? zi + blk * ZB + t * TS + kx : gi + blk * B * X + kx;
             float re[B], im[B];
 #pragma unroll
             for (int y = 0; y < B; ++y) {
@@ -314,19 +343,19 @@ __global__ void __launch_bounds__(256) dfttest_adjoint_kernel(const __grid_const
             __syncthreads();
             for (int task = tid; task < NBLK * B * X; task += L::NTH) {  // DFT_t of every (ky, kx)
                 const int blk = task / (B * X), bin = task - blk * (B * X);
-                float* pr = zr + blk * SPEC + bin;
-                float* pi = zi + blk * SPEC + bin;
+                float* pr = zr + blk * ZB + bin;
+                float* pi = zi + blk * ZB + bin;
                 float re[T], im[T];
 #pragma unroll
                 for (int t = 0; t < T; ++t) {
-                    re[t] = pr[t * B * X];
-                    im[t] = pi[t * B * X];
+                    re[t] = pr[t * TS];
+                    im[t] = pi[t * TS];
                 }
                 cdft_n<T>(re, im, false);
 #pragma unroll
                 for (int t = 0; t < T; ++t) {
-                    pr[t * B * X] = re[t];
-                    pi[t * B * X] = im[t];
+                    pr[t * TS] = re[t];
+                    pi[t * TS] = im[t];
                 }
             }
         }
@@ -334,8 +363,8 @@ __global__ void __launch_bounds__(256) dfttest_adjoint_kernel(const __grid_const
 
         // ---- through the gain and the zero-mean offset; thread owns bins gj + k GT of block gblk
         {
-            float* br = zr + gblk * SPEC;
-            float* bi = zi + gblk * SPEC;
+            float* br = zr + gblk * ZB;
+            float* bi = zi + gblk * ZB;
             const float* cr = gr + gblk * B * X;
             const float* ci = gi + gblk * B * X;
             const float g = a.zero_mean ? br[0] / wf0 : 0.0f;
@@ -348,20 +377,21 @@ __global__ void __launch_bounds__(256) dfttest_adjoint_kernel(const __grid_const
                     const int i = gj + k * GT;
                     if (SPEC % GT == 0 || i < SPEC) {
                         const int kt = i / (B * X), bin = i - kt * (B * X);
+                        const int zi_ = kt * TS + bin;  // index in the padded spectra
                         const float cs = s_tw[2 * kt], sn = s_tw[2 * kt + 1];
                         const float Gr = cr[bin] * cs - ci[bin] * sn;
                         const float Gi = cr[bin] * sn + ci[bin] * cs;
                         const float wr = s_wf[2 * i], wi = s_wf[2 * i + 1];
-                        const float dr = br[i] - g * wr, di = bi[i] - g * wi;
+                        const float dr = br[zi_] - g * wr, di = bi[zi_] - g * wi;
                         float m, dpsd, dsig;
                         gain_grad<FT>(dr * dr + di * di, s_sig[i], a, m, dpsd, dsig);
                         const float q = Gr * dr + Gi * di;
                         const float ddr = m * Gr + 2.0f * dpsd * q * dr;
                         const float ddi = m * Gi + 2.0f * dpsd * q * di;
-                        acc[k] += dsig * q;
+                        if (a.gsigma && dsig != 0.0f) atomicAdd(&s_gs[i], dsig * q);
                         dg += (Gr * wr + Gi * wi) - (ddr * wr + ddi * wi);
-                        br[i] = ddr;
-                        bi[i] = ddi;
+                        br[zi_] = ddr;
+                        bi[zi_] = ddi;
                     }
                 }
             };
@@ -380,26 +410,26 @@ __global__ void __launch_bounds__(256) dfttest_adjoint_kernel(const __grid_const
             if ((tid & (RW - 1)) == 0) atomicAdd(&s_dg[gblk], dg);
         }
         __syncthreads();
-        if (a.zero_mean && tid < NBLK) zr[tid * SPEC] += s_dg[tid] / wf0;
+        if (a.zero_mean && tid < NBLK) zr[tid * ZB] += s_dg[tid] / wf0;
 
         // ---- adjoint of the forward transform: inverse over t and y, halved c2r over x
         if constexpr (T > 1) {
             __syncthreads();
             for (int task = tid; task < NBLK * B * X; task += L::NTH) {
                 const int blk = task / (B * X), bin = task - blk * (B * X);
-                float* pr = zr + blk * SPEC + bin;
-                float* pi = zi + blk * SPEC + bin;
+                float* pr = zr + blk * ZB + bin;
+                float* pi = zi + blk * ZB + bin;
                 float re[T], im[T];
 #pragma unroll
                 for (int t = 0; t < T; ++t) {
-                    re[t] = pr[t * B * X];
-                    im[t] = pi[t * B * X];
+                    re[t] = pr[t * TS];
+                    im[t] = pi[t * TS];
                 }
                 cdft_n<T>(re, im, true);
 #pragma unroll
                 for (int t = 0; t < T; ++t) {
-                    pr[t * B * X] = re[t];
-                    pi[t * B * X] = im[t];
+                    pr[t * TS] = re[t];
+                    pi[t * TS] = im[t];
                 }
             }
         }
@@ -407,8 +437,8 @@ __global__ void __launch_bounds__(256) dfttest_adjoint_kernel(const __grid_const
         for (int task = tid; task < NBLK * T * X; task += L::NTH) {
             const int blk = task / (T * X), rem = task - blk * (T * X);
             const int t = rem / X, kx = rem - t * X;
-            float* pr = zr + blk * SPEC + t * B * X + kx;
-            float* pi = zi + blk * SPEC + t * B * X + kx;
+            float* pr = zr + blk * ZB + t * TS + kx;
+            float* pi = zi + blk * ZB + t * TS + kx;
             float re[B], im[B];
 #pragma unroll
             for (int y = 0; y < B; ++y) {
@@ -426,8 +456,8 @@ __global__ void __launch_bounds__(256) dfttest_adjoint_kernel(const __grid_const
         for (int task = tid; task < NBLK * T * B; task += L::NTH) {
             const int blk = task / (T * B), rem = task - blk * (T * B);
             const int t = rem / B, y = rem - t * B;
-            const float* pr = zr + blk * SPEC + (t * B + y) * X;
-            const float* pi = zi + blk * SPEC + (t * B + y) * X;
+            const float* pr = zr + blk * ZB + t * TS + y * X;
+            const float* pi = zi + blk * ZB + t * TS + y * X;
             float v[B], o[B];
             v[0] = pr[0];
             v[1] = pr[B / 2];
@@ -437,38 +467,28 @@ __global__ void __launch_bounds__(256) dfttest_adjoint_kernel(const __grid_const
                 v[2 * k + 1] = 0.5f * pi[k];
             }
             c2r_n<B>(v, o);
-            float* dst = dxp + (t * PH + (blk / TBX) * S + y) * PW + (blk % TBX) * S;
+            float* dst = dxp + (t * PH + (blk / TBX) * S + y) * PP + (blk % TBX) * S;
 #pragma unroll
             for (int x = 0; x < B; ++x) atomicAdd(dst + x, s_win[(t * B + y) * B + x] * o[x]);
         }
         __syncthreads();
 
         // ---- transposed gather: the patch back through the mirror into the source gradients
-        const int py0 = by0 * S, px0 = bx0 * S;
-        for (int i = tid; i < npatch; i += L::NTH) {
+        for (int i = tid; i < T * PH * PW; i += L::NTH) {
             const int t = i / (PH * PW), rem = i - t * (PH * PW);
             const int r = rem / PW, c = rem - r * PW;
             const int py = py0 + r, px = px0 + c;
-            const float v = dxp[i];
-            dxp[i] = 0.0f;
+            const float v = dxp[(t * PH + r) * PP + c];
             if (py < ph && px < pw && v != 0.0f)
                 atomicAdd(job.gsrc[t] + (long long)mirror(py - oy, Hh) * job.gsrc_stride + mirror(px - ox, W), v);
         }
     }
 
-    // ---- sigma gradient: per-thread partials -> shared -> global
+    // ---- sigma gradient: the CTA's partials -> global
     if (a.gsigma) {
         __syncthreads();
-        for (int i = tid; i < SPEC; i += L::NTH) zr[i] = 0.0f;
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < L::NPER; ++k) {
-            const int i = gj + k * GT;
-            if ((SPEC % GT == 0 || i < SPEC) && acc[k] != 0.0f) atomicAdd(&zr[i], acc[k]);
-        }
-        __syncthreads();
         for (int i = tid; i < SPEC; i += L::NTH)
-            if (zr[i] != 0.0f) atomicAdd(&a.gsigma[i], zr[i]);
+            if (s_gs[i] != 0.0f) atomicAdd(&a.gsigma[i], s_gs[i]);
     }
 }
 

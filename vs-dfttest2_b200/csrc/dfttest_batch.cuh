@@ -127,7 +127,7 @@ int prepare_group(dfttest2_b200_batch* b, dfttest2_b200_batch::Group& g, int var
     }
     g.smem = smem;
     KernelFn kern = g.generic ? var.generic : var.main;
-    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (int rc = prepare_kernel((const void*)kern, smem, var.nw * 32, nullptr)) return rc;
     if (g.d_jobs) CUDA_TRY(cudaFree(g.d_jobs));
     if (g.d_scratch) CUDA_TRY(cudaFree(g.d_scratch));
     if (g.d_seams) CUDA_TRY(cudaFree(g.d_seams));

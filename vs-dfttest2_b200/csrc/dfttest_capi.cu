@@ -40,6 +40,49 @@ int dft2h::fail(int code, const std::string& msg) {
     return code;
 }
 
+int dft2h::prepare_kernel(const void* kern, size_t smem, int threads, int* per_sm) {
+    // the limit only ever grows (every launch of the kernel, whatever its
+    // size, stays within it); occupancy is cached per launch shape
+    struct Limit {
+        int dev;
+        const void* kern;
+        size_t smem;
+    };
+    struct Occ {
+        int dev;
+        const void* kern;
+        size_t smem;
+        int threads;
+        int per_sm;
+    };
+    static std::mutex lock;
+    static std::vector<Limit> limits;
+    static std::vector<Occ> occ;
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(lock);
+    Limit* lim = nullptr;
+    for (Limit& l : limits)
+        if (l.dev == dev && l.kern == kern) lim = &l;
+    if (!lim || lim->smem < smem) {
+        CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if (lim) lim->smem = smem;
+        else limits.push_back(Limit{dev, kern, smem});
+    }
+    if (!per_sm) return 0;
+    for (const Occ& e : occ)
+        if (e.dev == dev && e.kern == kern && e.smem == smem && e.threads == threads) {
+            *per_sm = e.per_sm;
+            return 0;
+        }
+    int n = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, smem));
+    if (occ.size() > 4096) occ.clear();
+    occ.push_back(Occ{dev, kern, smem, threads, n});
+    *per_sm = n;
+    return 0;
+}
+
 dft2h::Variant dft2h::unit_variant(int B, int T, int NW, int MINB) {
     switch (B) {
     case 8: return unit_variant_b8(T, NW, MINB);
@@ -538,10 +581,9 @@ int launch_tc(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, f
     const size_t smem = v.smem(patch_w);
     if (smem > 227 * 1024) return fail(DFTTEST2_B200_EINVAL, "block step too large for the tensor-core form");
     TcKernelFn kern = f->filter_type == 0 ? v.wiener : v.generic;
-    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     int per_sm = 0;
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
+    if (int rc = prepare_kernel((const void*)kern, smem, 256, &per_sm)) return rc;
     if (per_sm < 1) return fail(DFTTEST2_B200_ECUDA, "tensor-core kernel does not fit on an SM");
     // two CTAs per SM (register bound of the kernel; tensor memory holds 2 x 256 columns); the occupancy
     // query can report one for this shared-memory size while two are resident, so it is not used for the grid
@@ -736,13 +778,10 @@ int launch(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, floa
         a.stage_off = (int)((smem_base + 127) & ~(size_t)127);
     }
     KernelFn kern = (f->filter_type == 0 && !f->asym && !sig_override) ? f->var.main : f->var.generic;
-    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    if (int rc = prepare_kernel((const void*)kern, smem, f->var.nw * 32, &per_sm)) return rc;
     int grid = plan.nunits;
-    if (persistent) {  // one CTA per resident slot
-        int per_sm = 0;
-        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, f->var.nw * 32, smem));
-        grid = std::min(plan.nunits, std::max(1, per_sm) * f->num_sms);
-    }
+    if (persistent) grid = std::min(plan.nunits, std::max(1, per_sm) * f->num_sms);  // one CTA per resident slot
     kern<<<grid, f->var.nw * 32, smem, stream>>>(a);
     CUDA_TRY(cudaGetLastError());
     if (plan.nfix > 0 && !inline_seams) {
@@ -1849,7 +1888,7 @@ extern "C" int dfttest2_b200_process_plane_noalloc(const dfttest2_b200_params* p
 
     const size_t smem = var.smem(a.ring_pitch);
     KernelFn kern = (p->filter_type == 0 && !asym) ? var.main : var.generic;
-    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (int rc = prepare_kernel((const void*)kern, smem, var.nw * 32, nullptr)) return rc;
     kern<<<a.nunits, var.nw * 32, smem, st>>>(a);
     CUDA_TRY(cudaGetLastError());
     if (a.nfix > 0) {

@@ -21,6 +21,12 @@ namespace dft2h {
 // records the message of a failing call for dfttest2_b200_last_error (per thread)
 int fail(int code, const std::string& msg);
 
+// Raises the kernel's dynamic shared-memory limit to `smem` (once per
+// device, kernel and size) and, when per_sm is given, returns its resident
+// CTAs per SM for `threads` threads (cached: the runtime queries cost more
+// than a small launch).
+int prepare_kernel(const void* kern, size_t smem, int threads, int* per_sm);
+
 #define CUDA_TRY(expr)                                                                                   \
     do {                                                                                                 \
         cudaError_t e_ = (expr);                                                                         \

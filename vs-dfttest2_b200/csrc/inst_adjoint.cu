@@ -27,9 +27,8 @@ int launch_adjoint_t(dft2::AdjointArgs a, int num_sms, cudaStream_t st) {
     a.patch_w = B + (L::TBX - 1) * a.block_step;
     const size_t smem = L::smem_bytes(a.patch_h, a.patch_w);
     auto kern = dft2::dfttest_adjoint_kernel<B, T>;
-    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, L::NTH, smem));
+    if (int rc = prepare_kernel((const void*)kern, smem, L::NTH, &per_sm)) return rc;
     if (per_sm < 1) return fail(DFTTEST2_B200_ECUDA, "adjoint kernel does not fit on an SM");
     const int grid = std::max(1, std::min(a.ntiles, num_sms * per_sm));
     kern<<<grid, L::NTH, smem, st>>>(a);
