@@ -761,9 +761,14 @@ int launch(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, floa
     a.error_flag = slot.d_error;
     // full-height strips: the unit kernel sums its seams itself
     const bool inline_seams = plan.nfix > 0 && plan.full_strips && plan.nseams > 0;
-    // persistent grid (a work counter after the seam counters; both zeroed by one memset)
+    // Persistent grid (a work counter after the seam counters; both zeroed by
+    // one memset) for launches of full-height strips, whose units are long;
+    // launches of strip segments (short units) run one unit per CTA, which
+    // measured 14 % faster there (the block scheduler balances as well, with
+    // less per-unit synchronisation).  DFTTEST2_B200_PERSISTENT=0 / 1 forces
+    // either.
     const char* penv = std::getenv("DFTTEST2_B200_PERSISTENT");
-    const bool persistent = !(penv && std::atoi(penv) == 0);
+    const bool persistent = penv ? std::atoi(penv) != 0 : plan.full_strips;
     if (inline_seams || persistent) {
         const size_t ncount = (size_t)(inline_seams ? plan.nseams : 0) + 1;
         if (int rc = ensure(slot.d_seams, slot.seams_cap, ncount, slot.done)) return rc;
