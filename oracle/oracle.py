@@ -4,6 +4,9 @@
   gcc_source/kernel.hpp, compiled unchanged by oracle/Makefile into
   oracle/_ref/libdfttest_ref.so, driven by oracle/ref_harness.cpp).  B=16
   only, FP32, with dfttest2_cpu's rounding and output conversion.
+* ``ref_cufft_plane`` -- the reference's general-block-size GPU path
+  (cuda_source/kernels.cu of vs-dfttest2 compiled unchanged, with cuFFT;
+  oracle/ref_cufft.cu), the checker for block sizes 8 and 32.
 * ``fp64_plane``  -- oracle/dfttest_oracle.c, an FP64 restatement of the
   same pipeline for any block size / radius; returns un-rounded values.
 
@@ -102,6 +105,45 @@ def _load_ref():
         ]
         _ref = lib
     return _ref
+
+
+REF_CUFFT_LIB = os.path.join(HERE, "_ref", "libdfttest_ref_cufft.so")
+_ref_cufft = None
+
+
+def ref_cufft_available() -> bool:
+    return os.path.exists(REF_CUFFT_LIB)
+
+
+def ref_cufft_plane(frames, args: dict, bits: int) -> np.ndarray:
+    """Output of the reference's cuFFT GPU path (cuda_source/kernels.cu +
+    cuFFT, oracle/ref_cufft.cu) for one plane, any block size; runs on the
+    current CUDA device.  Synthesis window slice r, as that backend."""
+    global _ref_cufft
+    if _ref_cufft is None:
+        lib = ctypes.CDLL(REF_CUFFT_LIB)
+        lib.ref_cufft_plane.restype = c_int
+        lib.ref_cufft_plane.argtypes = [
+            POINTER(c_void_p), c_int, c_int, c_int, c_int, c_int, c_void_p, c_int, POINTER(c_double),
+            POINTER(c_double), c_int, c_double, c_double, c_double, c_int, c_int, POINTER(c_double), c_int, c_int,
+            c_int,
+        ]
+        _ref_cufft = lib
+    src = [np.ascontiguousarray(f) for f in frames]
+    h, w = src[0].shape
+    out = np.empty_like(src[0])
+    ptrs = (c_void_p * len(src))(*[a.ctypes.data for a in src])
+    win, win_p = _dbl(args["window"])
+    sig, sig_p = _dbl(args["sigma"])
+    wf_vals = args["window_freq"] if args["window_freq"] is not None else np.zeros(1)
+    wf, wf_p = _dbl(wf_vals)
+    st = 1 if src[0].dtype == np.float32 else 0
+    rc = _ref_cufft.ref_cufft_plane(ptrs, w, h, w, st, 32 if st else bits, out.ctypes.data, w, win_p, sig_p,
+                                    len(sig), args["sigma2"], args["pmin"], args["pmax"], args["filter_type"],
+                                    args["zero_mean"], wf_p, args["radius"], args["block_size"], args["block_step"])
+    if rc != 0:
+        raise RuntimeError(f"reference cuFFT path failed ({rc})")
+    return out
 
 
 def _dbl(values) -> ctypes.Array:
