@@ -994,6 +994,102 @@ __device__ __noinline__ void stage_rows_plain(float* __restrict__ s_in, const St
     }
 }
 
+// Where a final overlap-add pixel goes: the output plane (pixels of the
+// unit's exclusive zone), or the unit's band record (pixels it shares).
+struct FinishGeom {
+    void* dst;
+    long long dst_stride;
+    int kind;
+    float scale, peak, inv_scale;  // inv_scale 0: float output (IEEE division by scale)
+    int x0, ox, oy, W, H;
+    int excl_x0, excl_x1, excl_y0, excl_y1;
+    float* rec;
+    int fw, fh, ry0, O, rec_stride;
+    int* err;
+};
+
+__device__ __forceinline__ void finish_px(const FinishGeom& g, int py, int lx, float v) {
+    const int px = g.x0 + lx;
+    if (px < g.ox || px >= g.ox + g.W || py < g.oy || py >= g.oy + g.H) return;
+    if (px >= g.excl_x0 && px < g.excl_x1 && py >= g.excl_y0 && py < g.excl_y1) {
+        store_sample(g.dst, (long long)(py - g.oy) * g.dst_stride + (px - g.ox), v, g.kind, g.scale, g.peak,
+                     g.inv_scale);
+    } else {
+        const int bi = band_index(lx, py - g.ry0, g.fw, g.fh, g.O);
+        if (DFT_IN_RANGE(bi, g.rec_stride, g.err)) g.rec[bi] = v;
+    }
+}
+
+// Overlap-add of one step for block steps that are not multiples of 4
+// (pixel items, any number of covering blocks); out of line, so that the
+// unit kernel's step loop carries only the 4-pixel segment path.
+template <int B, int T, int NW>
+__device__ __noinline__ void ola_scalar(const FinishGeom g, float* __restrict__ s_ola,
+                                        const float* __restrict__ s_wbuf, int pitch, int rowlen, int by, int S, int nbx,
+                                        int nfin, int tid) {
+    using L = Layout<B, T, NW>;
+    using TL = Tile<B>;
+    constexpr int NT = NW * 32;
+    const float inv_rl = 1.0f / (float)rowlen, inv_S = 1.0f / (float)S;
+    for (int i = tid; i < B * rowlen; i += NT) {
+        const int r = div_small(i, inv_rl), px = i - r * rowlen;
+        // blocks k with k*S <= px <= k*S + B - 1
+        const int b_lo = px <= B - 1 ? 0 : div_small(px - B + S, inv_S);
+        const int b_hi = min(div_small(px, inv_S), nbx - 1);
+        const int py = by * S + r;
+        float* cell = s_ola + (py & (B - 1)) * pitch + px;
+        float acc = *cell;
+        for (int k = b_lo; k <= b_hi; ++k) acc += s_wbuf[k * L::BSTR + TL::off(r, px - k * S)];
+        if (r < nfin) {
+            finish_px(g, py, px, acc);
+            acc = 0.0f;
+        }
+        *cell = acc;
+    }
+}
+
+// Seams shared by neighbouring full-height strips (launches with
+// KernelArgs::seam_count): the second of the two strips to finish sums both
+// band records (left strip first, as the fix-up kernel does) and stores the
+// result.  Nothing waits, so this is safe for any launch order.  Out of line
+// (runs once per unit).
+template <int B>
+__device__ __noinline__ void sum_seams(const KernelArgs& a, const PlaneJob& job, const FilterParams& P, int sx, int pnx,
+                                       int pny, int ox, int oy, int W, int Hh, float inv_scale, int tid, int NT) {
+    const int S = a.block_step, O = B - S;
+    __shared__ int s_arrival;
+    __threadfence();  // this unit's band records are visible before it arrives
+    __syncthreads();
+#pragma unroll 1
+    for (int side = 0; side < 2; ++side) {
+        const int k = side == 0 ? sx - 1 : sx;  // seam k lies between strips k and k + 1
+        if (k < 0 || k >= job.nsx - 1) continue;
+        if (tid == 0) s_arrival = atomicAdd(a.seam_count + job.seam_base + k, 1);
+        __syncthreads();
+        const bool second = (s_arrival == 1);
+        __syncthreads();
+        if (!second) continue;
+        __threadfence();
+        const UnitGeom ul = unit_geom(k, 0, job.nsx, 1, pnx, pny, B, S);
+        const UnitGeom ur = unit_geom(k + 1, 0, job.nsx, 1, pnx, pny, B, S);
+        const float* recl = a.scratch + (size_t)(job.unit_base + k) * a.rec_stride;
+        const float* recr = a.scratch + (size_t)(job.unit_base + k + 1) * a.rec_stride;
+        const int pxs = ur.bx0 * S;  // first padded column of the seam
+        for (int i = tid; i < O * Hh; i += NT) {
+            const int r = i / O;
+            const int py = oy + r, px = pxs + (i - r * O);
+            if (px < ox || px >= ox + W) continue;
+            const int il = band_index(px - ul.bx0 * S, py - ul.by0 * S, ul.fw, ul.fh, O);
+            const int ir = band_index(px - ur.bx0 * S, py - ur.by0 * S, ur.fw, ur.fh, O);
+            if (!DFT_IN_RANGE(il, a.rec_stride, a.error_flag) || !DFT_IN_RANGE(ir, a.rec_stride, a.error_flag))
+                continue;
+            const float v = 0.0f + __ldcg(recl + il) + __ldcg(recr + ir);
+            store_sample(job.dst, (long long)(py - oy) * job.dst_stride + (px - ox), v, P.kind, P.scale, P.peak,
+                         inv_scale);
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // main kernel
 // ---------------------------------------------------------------------------
@@ -1162,8 +1258,6 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
     const int excl_y0 = u.by0 * S + O, excl_y1 = u.by1 * S;
     const int excl_x0 = x0 + O, excl_x1 = u.bx1 * S;
 
-    const float inv_rl = 1.0f / (float)rowlen;
-    const float inv_S = 1.0f / (float)S;
     const StageGeom sgeo{job.src, job.src_stride, P.kind, rowlen, pitch, x0, ox, oy, W, Hh, a.error_flag};
     // prologue: the first B rows of the unit
     stage_rows_plain<B, T, NT>(s_in, sgeo, u.by0 * S, B, tid);
@@ -1224,17 +1318,10 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
         // ---- overlap-add of this step's blocks into the ring; rows that no
         // later block reaches are final and leave the ring (same thread, no barrier)
         const int nfin = last ? B : S;
-        auto finish = [&](int py, int lx, float v) {
-            const int px = x0 + lx;
-            if (px < ox || px >= ox + W || py < oy || py >= oy + Hh) return;
-            if (px >= excl_x0 && px < excl_x1 && py >= excl_y0 && py < excl_y1) {
-                store_sample(job.dst, (long long)(py - oy) * job.dst_stride + (px - ox), v, P.kind, P.scale, P.peak,
-                             is_float ? 0.0f : inv_scale);
-            } else {
-                const int bi = band_index(lx, py - u.by0 * S, fw, u.fh, O);
-                if (DFT_IN_RANGE(bi, a.rec_stride, a.error_flag)) rec[bi] = v;
-            }
-        };
+        const FinishGeom fg{job.dst, job.dst_stride, P.kind, P.scale, P.peak, is_float ? 0.0f : inv_scale,
+                            x0, ox, oy, W, Hh, excl_x0, excl_x1, excl_y0, excl_y1, rec, fw, u.fh, u.by0 * S, O,
+                            a.rec_stride, a.error_flag};
+        auto finish = [&](int py, int lx, float v) { finish_px(fg, py, lx, v); };
         if (vec) {
             // segment items (see ola_item): ring cell + covering blocks in ascending order
             auto do_item = [&](int it) {
@@ -1295,21 +1382,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
                 if (ola_it[j] >= 0) do_item(ola_it[j]);
             for (int i = tid + OJ * NT; i < n_ola; i += NT) do_item(ola_item(i));
         } else {
-            for (int i = tid; i < B * rowlen; i += NT) {
-                const int r = div_small(i, inv_rl), px = i - r * rowlen;
-                // blocks k with k*S <= px <= k*S + B - 1
-                const int b_lo = px <= B - 1 ? 0 : div_small(px - B + S, inv_S);
-                const int b_hi = min(div_small(px, inv_S), nbx - 1);
-                const int py = by * S + r;
-                float* cell = s_ola + (py & (B - 1)) * pitch + px;
-                float acc = *cell;
-                for (int k = b_lo; k <= b_hi; ++k) acc += s_wbuf[k * L::BSTR + TL::off(r, px - k * S)];
-                if (r < nfin) {
-                    finish(py, px, acc);
-                    acc = 0.0f;
-                }
-                *cell = acc;
-            }
+            ola_scalar<B, T, NW>(fg, s_ola, s_wbuf, pitch, rowlen, by, S, nbx, nfin, tid);
         }
 
         // ---- the next step's new input rows: by plain loads (planes the TMA copies cannot take)
@@ -1355,42 +1428,8 @@ __global__ void __launch_bounds__(NW * 32, MINB) dfttest_unit_kernel(const __gri
         }
     }
 
-    // ---- seams shared with the neighbouring full-height strips: the second of
-    // the two strips to finish sums both band records (left strip first, as
-    // the fix-up kernel does) and stores the result
-    if (a.seam_count != nullptr) {
-        __shared__ int s_arrival;
-        __threadfence();  // this unit's band records are visible before it arrives
-        __syncthreads();
-#pragma unroll 1
-        for (int side = 0; side < 2; ++side) {
-            const int k = side == 0 ? sx - 1 : sx;  // seam k lies between strips k and k + 1
-            if (k < 0 || k >= job.nsx - 1) continue;
-            if (tid == 0) s_arrival = atomicAdd(a.seam_count + job.seam_base + k, 1);
-            __syncthreads();
-            const bool second = (s_arrival == 1);
-            __syncthreads();
-            if (!second) continue;
-            __threadfence();
-            const UnitGeom ul = unit_geom(k, 0, job.nsx, 1, pnx, pny, B, S);
-            const UnitGeom ur = unit_geom(k + 1, 0, job.nsx, 1, pnx, pny, B, S);
-            const float* recl = a.scratch + (size_t)(job.unit_base + k) * a.rec_stride;
-            const float* recr = a.scratch + (size_t)(job.unit_base + k + 1) * a.rec_stride;
-            const int pxs = ur.bx0 * S;  // first padded column of the seam
-            for (int i = tid; i < O * Hh; i += NT) {
-                const int r = i / O;
-                const int py = oy + r, px = pxs + (i - r * O);
-                if (px < ox || px >= ox + W) continue;
-                const int il = band_index(px - ul.bx0 * S, py - ul.by0 * S, ul.fw, ul.fh, O);
-                const int ir = band_index(px - ur.bx0 * S, py - ur.by0 * S, ur.fw, ur.fh, O);
-                if (!DFT_IN_RANGE(il, a.rec_stride, a.error_flag) || !DFT_IN_RANGE(ir, a.rec_stride, a.error_flag))
-                    continue;
-                const float v = 0.0f + __ldcg(recl + il) + __ldcg(recr + ir);
-                store_sample(job.dst, (long long)(py - oy) * job.dst_stride + (px - ox), v, P.kind, P.scale, P.peak,
-                             is_float ? 0.0f : inv_scale);
-            }
-        }
-    }
+    // ---- seams shared with the neighbouring full-height strips
+    if (a.seam_count != nullptr) sum_seams<B>(a, job, P, sx, pnx, pny, ox, oy, W, Hh, is_float ? 0.0f : inv_scale, tid, NT);
 
     // ---- the next unit (persistent grid)
     if (a.unit_counter == nullptr) break;
