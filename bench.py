@@ -484,7 +484,7 @@ def main():
                     help="frames filtered frame by frame through the cached per-plane host path (0 skips)")
     ap.add_argument("--tc-steps", type=int, default=10,
                     help="steps timed for each tensor-core precision mode (0 skips the comparison)")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "tc_bf16x3", "tc_tf32", "tc_bf16"],
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "tc_fp16x3", "tc_bf16x3", "tc_tf32", "tc_bf16"],
                     help="arithmetic of the timed steps (profiling runs of the tensor-core form)")
     ap.add_argument("--extras", type=int, default=1,
                     help="0 skips the parity, differentiation and batching keys (profiling runs)")
@@ -591,13 +591,13 @@ def main():
     tc_results = {}
     if opts.tc_steps > 0 and opts.precision == "fp32":
         plain_out = [o.clone() for o in dev_out]
-        for mode in ("tc_bf16x3", "tc_tf32"):
+        for mode in ("tc_fp16x3", "tc_bf16x3", "tc_tf32"):
             flt.set_precision(mode)
             for _ in range(2):
                 step()
             torch.cuda.synchronize()
             flt.check()
-            if extras and mode == "tc_bf16x3":
+            if extras and mode in ("tc_fp16x3", "tc_bf16x3"):
                 parity[mode] = reference_parity(args, host_planes, dev_out, sample_frames, r)
             t_start, t_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             t_start.record(stream)

@@ -219,17 +219,23 @@ int dfttest2_b200_backward_planes(dfttest2_b200_filter* f, const dfttest2_b200_g
 /* Arithmetic of the per-block transforms.  FP32 (the default) runs them as
  * FP32 FFT codelets on the CUDA cores, like the reference's kernels
  * (nvrtc_source/kernels.cu:86-295).  The TC modes run them as dense products
- * on the tensor cores (tcgen05.mma, FP32 accumulation): TC_BF16X3 splits
- * every operand into bf16 hi + lo and sums three products (about 16
- * significant bits), TC_TF32 and TC_BF16 use one product (10 and 7 bits).
- * Available for block_size 16 with radius 0 or 1 and block_size 32 with
- * radius 0; the gain, zero-mean and overlap-add stay in FP32.  No
+ * on the tensor cores (tcgen05.mma, FP32 accumulation): TC_FP16X3 and
+ * TC_BF16X3 split every operand into 16-bit hi + lo parts and sum three
+ * products (about 22 and 16 significant bits), TC_TF32 and TC_BF16 use one
+ * product (10 and 7 bits); the gain, zero-mean and overlap-add stay in FP32.
+ * TC_FP16X3, and TC_BF16X3 where the arguments allow it, use the strip form
+ * (block_size 16, radius 0 or 1, block_step 1, 2 or 4, a separable window
+ * and sigma symmetric in the x-bins 0 and block_size/2, as the Python front
+ * end produces; the x products run over 8 blocks at once); TC_FP16X3 fails
+ * with DFTTEST2_B200_EINVAL outside it.  The other modes use the tile form
+ * (block_size 16 with radius 0 or 1, block_size 32 with radius 0).  No
  * counterpart in the reference.  Applies to the process_* paths of the
  * filter (not to the differentiable and batch paths, which stay FP32). */
 #define DFTTEST2_B200_FP32 0
 #define DFTTEST2_B200_TC_BF16X3 1
 #define DFTTEST2_B200_TC_TF32 2
 #define DFTTEST2_B200_TC_BF16 3
+#define DFTTEST2_B200_TC_FP16X3 4
 
 int dfttest2_b200_set_precision(dfttest2_b200_filter* f, int mode);
 

@@ -111,13 +111,18 @@ def test_yuv420p16_1080p_against_reference(yuv1080p, cuda_device):
         assert worst <= 1 and exact >= 0.99
 
 
-def test_yuv420p16_1080p_tensor_core_against_reference(yuv1080p, cuda_device):
+@pytest.mark.parametrize("mode", ["tc_fp16x3", "tc_bf16x3"])
+def test_yuv420p16_1080p_tensor_core_against_reference(yuv1080p, mode, cuda_device):
+    """The tensor-core strip form on the headline workload: within 1 LSB of the
+    reference CPU math; fp16 hi/lo (about 22 bits, FP32 accumulation in tensor
+    memory) also keeps >= 98 % of the samples exact (measured 98.8 %), bf16
+    hi/lo (about 16 bits) is only held to 1 LSB."""
     import torch
 
     planes, args, frames, ref = yuv1080p
     flt = Filter(device_id=0, **args)
     try:
-        flt.set_precision("tc_bf16x3")
+        flt.set_precision(mode)
         dev = [flt.process_clip_device(torch.from_numpy(p.view(np.int16)).cuda(0), 0, 16) for p in planes]
         flt.check()
         dev = [d.cpu().numpy().view(np.uint16) for d in dev]
@@ -130,5 +135,8 @@ def test_yuv420p16_1080p_tensor_core_against_reference(yuv1080p, cuda_device):
             worst = max(worst, m)
             exact_sum += e * dev[p][n].size
             count += dev[p][n].size
-    print(f"YUV420P16 1080p tensor-core bf16x3: max {worst} LSB vs reference, exact-match {exact_sum / count:.5f}")
+    exact = exact_sum / count
+    print(f"YUV420P16 1080p tensor-core {mode}: max {worst} LSB vs reference, exact-match {exact:.5f}")
     assert worst <= 1
+    if mode == "tc_fp16x3":
+        assert exact >= 0.98

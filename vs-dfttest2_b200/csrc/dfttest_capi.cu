@@ -263,6 +263,14 @@ struct dfttest2_b200_filter {
     int tc_mode = 0;
     void* d_gmat = nullptr;
     int gmat_bytes = 0;
+    // tensor-core strip form (dfttest_tc2.cuh): kernels, constant image, shape; tc2.main is
+    // null when the tensor-core mode runs the tile form of dfttest_tc.cuh instead
+    Variant tc2;
+    char* d_tc2 = nullptr;
+    Tc2Shape tc2_shape;
+    // plugin arrays kept on the host for the constant images of the tensor-core forms
+    std::vector<double> h_win, h_wf;
+    std::vector<float> h_sig;
     int wait_limit = dft2::kDefaultWaitLimit;  // iteration limit of the kernels' bounded device waits
 
     std::vector<Slot> slots;
@@ -514,8 +522,10 @@ int make_plan(const dfttest2_b200_filter* f, const dfttest2_b200_plane* planes, 
     // units go out in plan order: tall planes first (their strips are the
     // longest units), so that short units fill the last wave
     std::stable_sort(refs.begin(), refs.end(), [](const PlaneRef& x, const PlaneRef& y) { return x.height > y.height; });
-    const int BPS = strip_blocks(f->var, f->B, f->S);
-    const int nsy = choose_nsy(refs, f->B, f->S, BPS, std::max(1, f->var.minb) * f->num_sms);
+    const bool tc2 = f->tc_mode && f->tc2.main;
+    const int BPS = tc2 ? f->tc2_shape.nbx : strip_blocks(f->var, f->B, f->S);
+    const int minb = tc2 ? f->tc2.minb : f->var.minb;
+    const int nsy = choose_nsy(refs, f->B, f->S, BPS, std::max(1, minb) * f->num_sms);
     long long strips_total = 0;
     for (const PlaneRef& r : refs) strips_total += (dft2::pad_num(r.width, f->B, f->S) + BPS - 1) / BPS;
     // plan_units derives nsy = ceil(target / strips) = nsy from this target
@@ -702,7 +712,10 @@ void build_stage_maps(std::vector<dft2::PlaneJob>& jobs, const std::vector<int>&
 int launch(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, float scale, float peak,
            cudaStream_t stream, const float* sig_override = nullptr, const float* sig2_override = nullptr) {
     if (plan.nunits == 0) return 0;
-    if (f->tc_mode && !sig_override) return launch_tc(f, slot, plan, kind, scale, peak, stream);
+    // the tensor-core strip form runs in this framework; the tile form has its own launcher
+    const bool tc2 = f->tc_mode && f->tc2.main && !sig_override;
+    if (f->tc_mode && !sig_override && !tc2) return launch_tc(f, slot, plan, kind, scale, peak, stream);
+    const Variant& var = tc2 ? f->tc2 : f->var;
     CUDA_TRY(cudaStreamWaitEvent(stream, slot.done, 0));
     if (int rc = ensure(slot.d_jobs, slot.jobs_cap, plan.jobs.size(), slot.done)) return rc;
     const size_t scratch_need = (size_t)plan.nunits * plan.rec_stride;
@@ -712,9 +725,12 @@ int launch(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, floa
     std::vector<CUtensorMap> maps;
     int bw = 0;
     size_t stage = 0;
-    const size_t smem_base = f->var.smem(plan.pitch);
-    build_stage_maps(jobs, std::vector<int>(jobs.size(), kind), f->B, f->S, f->T, plan.pitch, maps, bw, stage,
-                     &slot.map_cache);
+    const size_t smem_base = tc2 ? f->tc2_shape.smem : f->var.smem(plan.pitch);
+    // the strip form reads 8 * xg footprint columns; its staging slots hold this launch's format
+    build_stage_maps(jobs, std::vector<int>(jobs.size(), kind), f->B, f->S, f->T,
+                     tc2 ? 8 * f->tc2_shape.xg : plan.pitch, maps, bw, stage, &slot.map_cache);
+    if (tc2 && bw > 0)
+        stage = (size_t)dft2::stage_bytes(bw, kind == dft2::kF32 ? 4 : (kind == dft2::kU16 ? 2 : 1), f->T, f->S) + 128;
     size_t smem = smem_base;
     if (bw > 0) {
         const size_t with_stage = ((smem_base + 127) & ~(size_t)127) + stage;
@@ -782,17 +798,21 @@ int launch(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, floa
         a.stage_bw = bw;
         a.stage_off = (int)((smem_base + 127) & ~(size_t)127);
     }
-    KernelFn kern = (f->filter_type == 0 && !f->asym && !sig_override) ? f->var.main : f->var.generic;
+    if (tc2) {
+        a.tc_consts = f->d_tc2;
+        a.wait_limit = f->wait_limit;
+    }
+    KernelFn kern = (f->filter_type == 0 && !f->asym && !sig_override) ? var.main : var.generic;
     int per_sm = 0;
-    if (int rc = prepare_kernel((const void*)kern, smem, f->var.nw * 32, &per_sm)) return rc;
+    if (int rc = prepare_kernel((const void*)kern, smem, var.nw * 32, &per_sm)) return rc;
     int grid = plan.nunits;
     if (persistent) grid = std::min(plan.nunits, std::max(1, per_sm) * f->num_sms);  // one CTA per resident slot
-    kern<<<grid, f->var.nw * 32, smem, stream>>>(a);
+    kern<<<grid, var.nw * 32, smem, stream>>>(a);
     CUDA_TRY(cudaGetLastError());
     if (plan.nfix > 0 && !inline_seams) {
         const int threads = 256;
         const int blocks = std::min((plan.nfix + threads - 1) / threads, f->num_sms * 8);
-        f->var.fixup<<<blocks, threads, 0, stream>>>(a);
+        var.fixup<<<blocks, threads, 0, stream>>>(a);
         CUDA_TRY(cudaGetLastError());
     }
     CUDA_TRY(cudaEventRecord(slot.done, stream));
@@ -980,6 +1000,7 @@ void free_filter(dfttest2_b200_filter* f) {
     cudaFree(f->d_sig_idx);
     cudaFree(f->d_sig2_idx);
     if (f->d_gmat) cudaFree(f->d_gmat);
+    if (f->d_tc2) cudaFree(f->d_tc2);
     delete f;
 }
 
@@ -1061,6 +1082,12 @@ int dfttest2_b200_create(const dfttest2_b200_params* p, dfttest2_b200_filter** o
     };
     f->wmask = wmask;
     f->asym = asym;
+    f->h_win.assign(p->window, p->window + T * B * B);
+    if (zero_mean) f->h_wf.assign(p->window_freq, p->window_freq + T * B * X * 2);
+    f->h_sig.resize(T * B * X);
+    for (int t = 0; t < T; ++t)
+        for (int y = 0; y < B; ++y)
+            for (int x = 0; x < X; ++x) f->h_sig[(t * B + y) * X + x] = sigma_at(t, y, x);
     f->g_div = zero_mean ? (float)p->window_freq[0] : 0.0f;
     if (zero_mean && f->g_div == 0.0f) return fail(DFTTEST2_B200_EINVAL, "window_freq[0] must be non-zero");
 
@@ -1126,15 +1153,44 @@ void dfttest2_b200_free(dfttest2_b200_filter* f) { free_filter(f); }
 
 int dfttest2_b200_set_precision(dfttest2_b200_filter* f, int mode) {
     if (!f) return fail(DFTTEST2_B200_EINVAL, "null filter");
-    if (mode < DFTTEST2_B200_FP32 || mode > DFTTEST2_B200_TC_BF16)
+    if (mode < DFTTEST2_B200_FP32 || mode > DFTTEST2_B200_TC_FP16X3)
         return fail(DFTTEST2_B200_EINVAL, "unknown precision mode");
     DeviceGuard dg(f->device);
     // no launch of this filter may still read the old constants
     for (Slot& s : f->slots)
         if (s.done) CUDA_TRY(cudaEventSynchronize(s.done));
-    if (mode == DFTTEST2_B200_FP32) {
-        f->tc_mode = 0;
-        return 0;
+    f->tc_mode = 0;
+    f->tc2 = Variant{};
+    if (mode == DFTTEST2_B200_FP32) return 0;
+    // the split-product modes run the strip form where the arguments allow it
+    // (DFTTEST2_B200_TC_STRIP=0 keeps BF16X3 on the tile form)
+    if (mode == DFTTEST2_B200_TC_FP16X3 || mode == DFTTEST2_B200_TC_BF16X3) {
+        const char* env = std::getenv("DFTTEST2_B200_TC_STRIP");
+        const bool allow = !(env && std::atoi(env) == 0) || mode == DFTTEST2_B200_TC_FP16X3;
+        std::string why = "the tensor-core strip form needs block_size 16";
+        const int fmt = mode == DFTTEST2_B200_TC_FP16X3 ? kTc2FmtFp16 : kTc2FmtBf16;
+        std::vector<char> img;
+        Tc2Shape shape;
+        int rc = 1;
+        if (f->asym) why = "the tensor-core strip form needs sigma symmetric in the x-bins 0 and B/2";
+        else if (f->B == 16 && allow) {
+            const Tc2Input in{f->T, f->S, f->radius, f->syn_slice, f->h_win.data(),
+                              f->zero_mean ? f->h_wf.data() : nullptr, f->h_sig.data(), fmt};
+            rc = tc2_build(in, img, shape, why);
+        }
+        if (rc == 0) {
+            if (f->d_tc2) CUDA_TRY(cudaFree(f->d_tc2));
+            f->d_tc2 = nullptr;
+            CUDA_TRY(cudaMalloc((void**)&f->d_tc2, img.size()));
+            CUDA_TRY(cudaMemcpy(f->d_tc2, img.data(), img.size(), cudaMemcpyHostToDevice));
+            f->tc2 = tc2_variant(f->T, fmt);
+            f->tc2_shape = shape;
+            for (KernelFn k : {f->tc2.main, f->tc2.generic})
+                CUDA_TRY(cudaFuncSetAttribute((const void*)k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+            f->tc_mode = mode;
+            return 0;
+        }
+        if (mode == DFTTEST2_B200_TC_FP16X3) return fail(DFTTEST2_B200_EINVAL, why);
     }
     const TcVariant v = select_tc(f->B, f->T, mode);
     if (!v.wiener)

@@ -74,4 +74,25 @@ struct TcVariant {
 TcVariant select_tc(int B, int T, int mode);
 int launch_tc_finalize(const dft2::TcArgs& a, dim3 grid, cudaStream_t st);
 
+// tensor-core strip form (inst_tc2.cu): 16x16 blocks, radius 0 or 1, block
+// steps 1, 2, 4, separable windows; runs in the unit framework (same plans,
+// band records, seams and fix-up kernel as the FP32 unit kernel)
+struct Tc2Input {
+    int T, S, radius, syn;
+    const double* window;  // [T][16][16]
+    const double* wfreq;   // [T][16][9][2] window spectrum, null without zero-mean
+    const float* sigma;    // [T][16][9]
+    int fmt;               // kTc2FmtFp16 / kTc2FmtBf16
+};
+constexpr int kTc2FmtFp16 = 0, kTc2FmtBf16 = 1;  // dft2::kTc2Fp16 / kTc2Bf16 of dfttest_tc2.cuh
+struct Tc2Shape {
+    int nbx = 0;       // blocks per strip
+    int xg = 0;        // 8-column groups of a strip footprint the kernel reads
+    size_t smem = 0;   // dynamic shared memory per CTA
+};
+// Builds the constant image; non-zero (with the reason) when the arguments
+// are outside the form.
+int tc2_build(const Tc2Input& in, std::vector<char>& img, Tc2Shape& shape, std::string& why);
+Variant tc2_variant(int T, int fmt);
+
 }  // namespace dft2h

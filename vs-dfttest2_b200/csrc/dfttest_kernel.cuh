@@ -167,6 +167,10 @@ struct KernelArgs {
     // gridDim.x + atomicAdd(unit_counter, 1) until none is left; the counter
     // is zeroed before the launch.  Null: one unit per CTA.
     int* unit_counter;
+    // constant image of the tensor-core strip form (dfttest_tc2.cuh) and the poll limit of its
+    // waits for the tensor cores; unused by the FP32 kernels
+    const char* tc_consts;
+    int wait_limit;
 };
 
 constexpr int kTmapBytes = 128;

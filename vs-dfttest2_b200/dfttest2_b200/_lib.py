@@ -109,7 +109,7 @@ class Clip(ctypes.Structure):
 BATCH_TUNE = 1
 
 # dfttest2_b200_set_precision modes
-PRECISION = {"fp32": 0, "tc_bf16x3": 1, "tc_tf32": 2, "tc_bf16": 3}
+PRECISION = {"fp32": 0, "tc_bf16x3": 1, "tc_tf32": 2, "tc_bf16": 3, "tc_fp16x3": 4}
 
 # every symbol include/dfttest2_b200.h declares, with its ctypes signature
 SIGNATURES = {

@@ -68,7 +68,7 @@ class Filter:
 
     def set_precision(self, mode: str) -> None:
         """Arithmetic of the block transforms: "fp32" (CUDA-core FFT codelets,
-        the default) or a tensor-core form "tc_bf16x3", "tc_tf32", "tc_bf16"
+        the default) or a tensor-core form "tc_fp16x3", "tc_bf16x3", "tc_tf32", "tc_bf16"
         (dfttest2_b200_set_precision)."""
         if mode not in _lib.PRECISION:
             raise Error(f"unknown precision mode {mode!r}; one of {sorted(_lib.PRECISION)}")
