@@ -783,8 +783,10 @@ int launch(dfttest2_b200_filter* f, Slot& slot, const Plan& plan, int kind, floa
     // measured 14 % faster there (the block scheduler balances as well, with
     // less per-unit synchronisation).  DFTTEST2_B200_PERSISTENT=0 / 1 forces
     // either.
+    // (the tensor-core strip form runs one unit per CTA: its persistent grid measured 1.6x slower on
+    // the 64-frame 1080p step, 42.1 against 25.7 ms)
     const char* penv = std::getenv("DFTTEST2_B200_PERSISTENT");
-    const bool persistent = penv ? std::atoi(penv) != 0 : plan.full_strips;
+    const bool persistent = penv ? std::atoi(penv) != 0 : plan.full_strips && !tc2;
     if (inline_seams || persistent) {
         const size_t ncount = (size_t)(inline_seams ? plan.nseams : 0) + 1;
         if (int rc = ensure(slot.d_seams, slot.seams_cap, ncount, slot.done)) return rc;
@@ -1183,7 +1185,7 @@ int dfttest2_b200_set_precision(dfttest2_b200_filter* f, int mode) {
             f->d_tc2 = nullptr;
             CUDA_TRY(cudaMalloc((void**)&f->d_tc2, img.size()));
             CUDA_TRY(cudaMemcpy(f->d_tc2, img.data(), img.size(), cudaMemcpyHostToDevice));
-            f->tc2 = tc2_variant(f->T, fmt);
+            f->tc2 = tc2_variant(f->T, fmt, f->S);
             f->tc2_shape = shape;
             for (KernelFn k : {f->tc2.main, f->tc2.generic})
                 CUDA_TRY(cudaFuncSetAttribute((const void*)k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));

@@ -93,6 +93,6 @@ struct Tc2Shape {
 // Builds the constant image; non-zero (with the reason) when the arguments
 // are outside the form.
 int tc2_build(const Tc2Input& in, std::vector<char>& img, Tc2Shape& shape, std::string& why);
-Variant tc2_variant(int T, int fmt);
+Variant tc2_variant(int T, int fmt, int S);
 
 }  // namespace dft2h

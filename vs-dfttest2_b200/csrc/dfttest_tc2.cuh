@@ -29,10 +29,15 @@
 //               over t of the centre frame (a sum, centre-first order);
 //   inverse x : 16-point complex IDFT per (blk, ky) on the CUDA cores
 //               (register codelet); the x synthesis window scales the output rows;
-//   inverse y : MMA_IY  D[(blk, x)][y] = Y'[(blk, x)][j] * Wiy[j][y]   (c2r
-//               over y, y synthesis window folded in);
-//   overlap-add of the block outputs in a shared-memory ring; final rows
-//   go to the output (or the unit's band record) as in the unit kernel.
+//   inverse y : MMA_IY  D[(blk, x)][row mod 16] += Y'[(blk, x)][j] * Wiy_rot[j][row mod 16]
+//               (c2r over y, y synthesis window folded in): the overlap-add
+//               in y happens in the tensor-memory accumulator, whose column
+//               of an output row is the row's index mod 16 (the constant's
+//               columns are rotated instead of moving the accumulator);
+//   overlap-add in x of the rows no later block row reaches (S rows a
+//   step): the columns are read, restarted from zero, and the blocks
+//   covering each 4-pixel segment summed; final pixels go to the output
+//   (or the unit's band record) as in the unit kernel.
 // Our bins are (ky 0..8, kx 0..15), the reference's (ky 0..15, kx 0..8):
 // a bin with kx > 8 is the conjugate of the reference bin (-kt, -ky, 16-kx),
 // whose sigma and window spectrum the gain table holds.
@@ -71,7 +76,6 @@ struct Tc2Head {
 };
 constexpr int kTc2HeadBytes = 256;
 constexpr int kTc2ZPitch = 18;       // float2 per (block, y-bin) row of the gain output (bank spread)
-constexpr int kTc2BlkStride = 260;   // floats per block of the block-output buffer (bank spread)
 static_assert(sizeof(Tc2Head) <= kTc2HeadBytes, "Tc2Head");
 
 // shared-memory plan (bytes from the 128-aligned dynamic base)
@@ -80,7 +84,6 @@ struct Tc2Smem {
     int ring, ring_hl;  // P ring: [hl][p][xg][16 rows x 16 B], + slack for the M rows past xg
     int yb, yb_hl;      // Y operand [hl][n-group][xg][8 rows x 16 B]; the gain output aliases it
     int ai, ai_tile;    // inverse-y operand [tile][hl][16 m-groups][2 x 128 B]
-    int ola;            // overlap-add ring [16 rows][xg * 8 floats]
     int total;
     __host__ __device__ static Tc2Smem make(int consts_bytes, int np, int xg) {
         Tc2Smem s;
@@ -94,9 +97,7 @@ struct Tc2Smem {
         const int yb_bytes = 2 * s.yb_hl > zbytes ? 2 * s.yb_hl : zbytes;
         s.ai = s.yb + ((yb_bytes + 127) & ~127);
         s.ai_tile = 2 * 16 * 256;
-        const int blk_bytes = 16 * kTc2BlkStride * 4;
-        s.ola = s.ai + (2 * s.ai_tile > blk_bytes ? 2 * s.ai_tile : blk_bytes);
-        s.total = s.ola + 16 * xg * 8 * 4;
+        s.total = s.ai + 2 * s.ai_tile;  // the final-row buffer (16 x 16 x 16 floats) aliases it
         return s;
     }
 };
@@ -149,11 +150,24 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float (&v)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16};" ::"r"(taddr),
+        "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3])),
+        "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])), "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])),
+        "r"(__float_as_uint(v[8])), "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])),
+        "r"(__float_as_uint(v[11])), "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])),
+        "r"(__float_as_uint(v[14])), "r"(__float_as_uint(v[15]))
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
 // packed real-DFT bin index of y-bin ky: j 0 = Re 0, 1 = Re 8, 2k = Re k, 2k + 1 = Im k
 __host__ __device__ constexpr int tc2_jre(int ky) { return ky == 0 ? 0 : (ky == 8 ? 1 : 2 * ky); }
 __host__ __device__ constexpr int tc2_jim(int ky) { return 2 * ky + 1; }
 
-template <int T, int FC, int FMT>
+template <int T, int FC, int FMT, int SS>
 __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_constant__ KernelArgs a) {
     constexpr int NT = 256;
     constexpr int NP = T;          // P planes
@@ -176,7 +190,8 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
         reinterpret_cast<int*>(&s_head)[tid] = reinterpret_cast<const int*>(gh)[tid];
     __syncthreads();
     const Tc2Head& hd = s_head;
-    const int S = hd.S, O = 16 - S, XG = hd.xg;
+    constexpr int S = SS, O = 16 - S;  // block step (the host built the constants for it)
+    const int XG = hd.xg;
     const Tc2Smem L = Tc2Smem::make(hd.total - hd.off_wy, NP, XG);
     {
         const uint4* src = reinterpret_cast<const uint4*>(a.tc_consts + hd.off_wy);
@@ -191,12 +206,10 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
     char* s_yb = tc2_smem + L.yb;
     float2* s_z = reinterpret_cast<float2*>(tc2_smem + L.yb);  // gain output, aliases the Y operand
     char* s_ai = tc2_smem + L.ai;
-    float* s_blk = reinterpret_cast<float*>(tc2_smem + L.ai);  // block outputs, after the inverse-y products
-    float* s_ola = reinterpret_cast<float*>(tc2_smem + L.ola);
-    const int opitch = XG * 8;  // floats per overlap-add ring row
+    // final output rows [row][block][x] (16 x 16 x 16 floats), after the inverse-y products
+    float* s_fin = reinterpret_cast<float*>(tc2_smem + L.ai);
     // the ring's slack rows are read (as M rows past the footprint) before any write: keep them finite
     for (int i = tid; i < (L.yb - L.ring) / 16; i += NT) reinterpret_cast<uint4*>(s_ring)[i] = make_uint4(0, 0, 0, 0);
-    for (int i = tid; i < 16 * opitch; i += NT) s_ola[i] = 0.0f;
     if (tid == 0) {
         // arrivals per batch: one commit per issuing thread (planes, x-product regions, tiles)
         mbar_init(&s_bars[0], NP);
@@ -225,9 +238,10 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
     tc_fence_after();
     const uint32_t tmem = s_tmem;
     const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
-    // tensor-memory columns: D_Y (and, later in a step, D_out) at 0; D_X tile h, part c at NJ + (2h + c) NJ
-    // (D_out spans 32 columns for two tiles: D_X starts past both D_Y and D_out)
-    constexpr uint32_t C_Y = 0, C_OUT = 0, C_X = NJ > 32 ? NJ : 32;
+    // tensor-memory columns: D_X tile h, part c at (2h + c) NJ; D_Y in the columns of tile 1 part sin
+    // (written after the gain has read them); D_out, the overlap-add accumulator of the inverse-y
+    // products (16 output rows, indexed by padded row mod 16, per tile), after D_X
+    constexpr uint32_t C_X = 0, C_Y = 3 * NJ, C_OUT = 4 * NJ;
     // one barrier per product batch; bit k of `ph` is the phase batch k waits for next
     constexpr int BY = 0, BX = 1, BIY = 2;
     uint32_t ph = 0;
@@ -421,19 +435,6 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
                 //      rows get theirs at the end of the previous iteration, with its overlap-add
                 if (it == u.by0)
                     for (int item = tid; item < 16 * ng4; item += NT) pconv_item(item, it * S, 16, 1.0f / 16.0f, false, 0);
-                // ---- 2. MMA_Y: D_Y[x][(p, j)] = ring_p[x][ring row] * Wy_rot[ring row][j]
-                to_tensor_cores();
-                if (issuer && warp < NP) {  // plane p = warp
-                    const int rot = ((it * S) & 15) / S;
-                    const uint32_t id = idesc2(FMT, 128, 16, true, false);
-                    const uint32_t wy = a_wy + rot * 2 * WY_BYTES;
-                    const uint32_t ap = a_ring + warp * XG * 256;
-                    const uint64_t da = sdesc(0, 128, 256);
-#pragma unroll
-                    for (int part = 0; part < 2; ++part)
-                        mma3(part, tmem + C_Y + 16 * warp, ap, ap + L.ring_hl, da, wy, wy + WY_BYTES, da, id, false);
-                    commit(BY);
-                }
             }
             if (back) {
                 // ---- 5. gain of block row bb: lane (blk, kx) of tile hf, every (kt, ky) bin of its block
@@ -517,8 +518,22 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
                         }
                     }
                 }
-                tc_fence_before();
-                __syncthreads();
+            }
+            // ---- 2. MMA_Y of block row it: D_Y[x][(p, j)] = ring_p[x][ring row] * Wy_rot[ring row][j], into the
+            //      columns of D_X tile 1 part sin, which the gain above has read (the barrier orders it)
+            to_tensor_cores();
+            if (front && issuer && warp < NP) {  // plane p = warp
+                const int rot = ((it * S) & 15) / S;
+                const uint32_t id = idesc2(FMT, 128, 16, true, false);
+                const uint32_t wy = a_wy + rot * 2 * WY_BYTES;
+                const uint32_t ap = a_ring + warp * XG * 256;
+                const uint64_t da = sdesc(0, 128, 256);
+#pragma unroll
+                for (int part = 0; part < 2; ++part)
+                    mma3(part, tmem + C_Y + 16 * warp, ap, ap + L.ring_hl, da, wy, wy + WY_BYTES, da, id, false);
+                commit(BY);
+            }
+            if (back) {
                 // ---- 6. inverse x per (block, y-bin): 16-point complex IDFT, x synthesis window -> inverse-y operand
                 if (tid < 16 * 9) {
                     const int b = tid / 9, ky = tid - b * 9;
@@ -573,20 +588,23 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
                     }
                 }
             }
-            // ---- 4 and 7. products: inverse y of block row bb (D_out aliases D_Y, read above), then the
-            //      x products of block row it
+            // ---- 4 and 7. products: inverse y of block row bb (accumulated into D_out), then the x
+            //      products of block row it (D_X, the Y products read above included)
             to_tensor_cores();
             if (issuer) {
                 if (back && warp < 2) {  // tile h = warp (an empty commit when the strip has one tile)
                     const int h = warp;
                     if (h < ntile) {
+                        // output row (bb S + y) of the block lands in accumulator column (bb S + y) mod 16:
+                        // the constant's columns are rotated; the unit's first block row starts the sums
                         const uint32_t id = idesc2(FMT, 128, 16, true, false);
                         const uint32_t ah = a_ai + h * L.ai_tile;
+                        const uint32_t wi = a_wi + (((bb * S) & 15) / S) * 2 * WY_BYTES;
                         const uint64_t da = sdesc(0, 128, 256);
 #pragma unroll
                         for (int part = 0; part < 2; ++part)
-                            mma3(part, tmem + C_OUT + 16 * h, ah, ah + 16 * 256, da, a_wi, a_wi + WY_BYTES, da, id,
-                                 false);
+                            mma3(part, tmem + C_OUT + 16 * h, ah, ah + 16 * 256, da, wi, wi + WY_BYTES, da, id,
+                                 bb > u.by0);
                     }
                     commit(BIY);
                 }
@@ -608,33 +626,50 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
                 }
             }
             if (back) {
-                // ---- 8. block outputs of block row bb -> block buffer (aliases the inverse-y operand)
+                // ---- 8. final rows of block row bb: the accumulator columns of the output rows that no
+                //      later block row reaches (S rows; all 16 at the unit's last block row), x synthesis
+                //      window, per block into the row buffer (aliases the inverse-y operand, which the
+                //      products have read); those columns restart from zero for the next block row
                 if (!wait_batch(BIY)) {
                     failed = true;
                     break;
                 }
                 {
+                    const bool last = (bb + 1 == u.by1);
+                    const int c0 = (bb * S) & 15;  // accumulator column of output row bb * S
                     const int l = quarter * 32 + lane;
                     const int blk = l >> 4, x = l & 15;
                     const int b = hf * 8 + blk;
+                    const uint32_t col = tmem + lane_base + C_OUT + 16 * hf;
                     float v[16];
-                    tmem_ld16(tmem + lane_base + C_OUT + 16 * (hf & 1), v);
+                    tmem_ld16(col, v);
                     tmem_wait_ld();
                     if (hf < ntile && b < nbx) {
-                        const float w = hd.sx[x];  // x synthesis window (rows of the inverse-y products)
+                        const float w = hd.sx[x];
 #pragma unroll
-                        for (int y = 0; y < 16; ++y) s_blk[b * kTc2BlkStride + y * 16 + x] = v[y] * w;
+                        for (int y = 0; y < 16; ++y) {  // column y holds output row bb S + ((y - c0) mod 16)
+                            const int r = (y - c0) & 15;
+                            if (last || r < S) s_fin[(r * 16 + b) * 16 + x] = v[y] * w;
+                        }
+                    }
+                    if (!last) {
+#pragma unroll
+                        for (int y = 0; y < 16; ++y)
+                            if (((y - c0) & 15) < S) v[y] = 0.0f;
+                        tmem_st16(col, v);
+                        tmem_wait_st();
                     }
                 }
                 tc_fence_before();
                 __syncthreads();
             }
-            // ---- 9. overlap-add of block row bb (item (row r, 4-pixel segment q): its ring cell plus the
-            //      covering blocks in ascending order; rows no later block row reaches are final and
-            //      leave the ring), and the P planes of block row it + 1 (its S new rows, staged or
-            //      plain loads), in one loop: the ring rows they overwrite were read by MMA_Y(it)
+            // ---- 9. output of block row bb's final rows (item (row r, 4-pixel segment q): the covering
+            //      blocks in ascending order), and the P planes of block row it + 1 (its S new rows,
+            //      staged or plain loads), in one loop: the ring rows they overwrite were read by MMA_Y(it)
             {
-                const int n_ola = back ? 16 * nseg : 0;
+                const bool last = (bb + 1 == u.by1);
+                const int nfin = last ? 16 : S;
+                const int n_out = back ? nfin * nseg : 0;
                 const bool next = it + 1 < u.by1;
                 const int n_pc = next ? S * 2 * XG : 0;
                 const bool staged = use_tma && next;
@@ -649,27 +684,23 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
                         mbar_wait(&s_sbar[slot], parity, 16 * kDefaultWaitLimit);
                     }
                 }
-                const bool last = (bb + 1 == u.by1);
-                const int nfin = last ? 16 : S;
-                for (int item = tid; item < n_ola + n_pc; item += NT) {
-                    if (item >= n_ola) {
-                        pconv_item(item - n_ola, (it + 1) * S + O, S, inv_S, staged, slot);
+                for (int item = tid; item < n_out + n_pc; item += NT) {
+                    if (item >= n_out) {
+                        pconv_item(item - n_out, (it + 1) * S + O, S, inv_S, staged, slot);
                         continue;
                     }
-
                     const int r = div_small(item, inv_nseg), q = item - r * nseg;
                     const int py = bb * S + r;
-                    float4* cell = reinterpret_cast<float4*>(s_ola + (py & 15) * opitch + 4 * q);
-                    float4 acc = *cell;
+                    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
                     float* av = reinterpret_cast<float*>(&acc);
-                    if ((S & 3) == 0) {
+                    const float* row = s_fin + r * 256;
+                    if constexpr ((S & 3) == 0) {
                         // the segment lies inside or outside each block
                         const int px = 4 * q;
                         const int b_lo = px + 4 <= 16 ? 0 : (px + 4 - 16 + S - 1) / S;
                         const int b_hi = min(px / S, nbx - 1);
                         for (int b = b_lo; b <= b_hi; ++b) {
-                            const float4 w4 =
-                                *reinterpret_cast<const float4*>(s_blk + b * kTc2BlkStride + r * 16 + (px - b * S));
+                            const float4 w4 = *reinterpret_cast<const float4*>(row + b * 16 + (px - b * S));
                             acc.x += w4.x;
                             acc.y += w4.y;
                             acc.z += w4.z;
@@ -681,26 +712,22 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
                             const int px = 4 * q + i;
                             const int b_lo = px <= 15 ? 0 : (px - 15 + S - 1) / S;
                             const int b_hi = min(px / S, nbx - 1);
-                            for (int b = b_lo; b <= b_hi; ++b) av[i] += s_blk[b * kTc2BlkStride + r * 16 + (px - b * S)];
+                            for (int b = b_lo; b <= b_hi; ++b) av[i] += row[b * 16 + (px - b * S)];
                         }
                     }
-                    if (r < nfin) {
-                        const int gx = x0 + 4 * q;
-                        if (4 * q + 4 <= u.fw && gx >= excl_x0 && gx + 4 <= excl_x1 && gx >= ox && gx + 4 <= ox + W &&
-                            py >= excl_y0 && py < excl_y1 && py >= oy && py < oy + Hh) {
-                            store4(job.dst, (long long)(py - oy) * job.dst_stride + (gx - ox), acc, P.kind, P.peak,
-                                   inv_scale);
-                        } else {
+                    const int gx = x0 + 4 * q;
+                    if (4 * q + 4 <= u.fw && gx >= excl_x0 && gx + 4 <= excl_x1 && gx >= ox && gx + 4 <= ox + W &&
+                        py >= excl_y0 && py < excl_y1 && py >= oy && py < oy + Hh) {
+                        store4(job.dst, (long long)(py - oy) * job.dst_stride + (gx - ox), acc, P.kind, P.peak,
+                               inv_scale);
+                    } else {
 #pragma unroll
-                            for (int i = 0; i < 4; ++i)
-                                if (4 * q + i < u.fw) finish_px(fg, py, 4 * q + i, av[i]);
-                        }
-                        acc = make_float4(0.f, 0.f, 0.f, 0.f);
+                        for (int i = 0; i < 4; ++i)
+                            if (4 * q + i < u.fw) finish_px(fg, py, 4 * q + i, av[i]);
                     }
-                    *cell = acc;
-                                }
+                }
             }
-            // the next iteration's first barrier orders these ring and block-buffer accesses before reuse
+            // the next iteration's first barrier orders these ring and row-buffer accesses before reuse
         }
         if (failed) break;
 

@@ -105,7 +105,7 @@ int tc2_build(const Tc2Input& in, std::vector<char>& img, Tc2Shape& shape, std::
     h.off_wy = dft2::kTc2HeadBytes;
     h.off_wx = align128(h.off_wy + wy_bytes);
     h.off_wi = align128(h.off_wx + 4 * wx_part);
-    h.off_tab = align128(h.off_wi + 1024);
+    h.off_tab = align128(h.off_wi + h.nrot * 1024);
     h.total = align128(h.off_tab + T * 9 * 16 * 16);
     img.assign((size_t)h.total, 0);
 
@@ -139,21 +139,24 @@ int tc2_build(const Tc2Input& in, std::vector<char>& img, Tc2Shape& shape, std::
             }
         }
     }
-    // inverse y (c2r over the packed bins j), y synthesis window: N = y, K = j
-    {
-        const size_t base = (size_t)h.off_wi;
-        for (int y = 0; y < B; ++y)
+    // inverse y (c2r over the packed bins j), y synthesis window: N = accumulator column c (output
+    // row y = (c - rot S) mod 16 of the block), K = j; one copy per rotation
+    for (int rot = 0; rot < h.nrot; ++rot) {
+        const size_t base = (size_t)h.off_wi + rot * 1024;
+        for (int c = 0; c < B; ++c) {
+            const int y = ((c - rot * S) % B + B) % B;
             for (int ky = 0; ky <= 8; ++ky) {
                 const double cw = (ky == 0 || ky == 8) ? 1.0 : 2.0;
                 const double th = 2.0 * kPi * (double)(ky * y % B) / B;
                 const int jr = dft2::tc2_jre(ky);
-                put_split(img, base + kmaj16(y, jr), base + 512 + kmaj16(y, jr), cw * std::cos(th) * sy[y], in.fmt);
+                put_split(img, base + kmaj16(c, jr), base + 512 + kmaj16(c, jr), cw * std::cos(th) * sy[y], in.fmt);
                 if (ky >= 1 && ky <= 7) {
                     const int ji = dft2::tc2_jim(ky);
-                    put_split(img, base + kmaj16(y, ji), base + 512 + kmaj16(y, ji), -cw * std::sin(th) * sy[y],
+                    put_split(img, base + kmaj16(c, ji), base + 512 + kmaj16(c, ji), -cw * std::sin(th) * sy[y],
                               in.fmt);
                 }
             }
+        }
     }
     // gain table [kt][ky 0..8][kx 0..15]: (sigma, window spectrum re, im) of the bin; a bin with
     // kx > 8 is the conjugate of the reference's bin (-kt, -ky, 16 - kx); the window spectrum is
@@ -196,22 +199,31 @@ int tc2_build(const Tc2Input& in, std::vector<char>& img, Tc2Shape& shape, std::
 }
 
 namespace {
-template <int T, int FMT>
+template <int T, int FMT, int S>
 Variant make_tc2() {
     Variant v;
-    v.main = dft2::dfttest_tc2_kernel<T, dft2::kFilterWiener, FMT>;
-    v.generic = dft2::dfttest_tc2_kernel<T, dft2::kFilterGeneric, FMT>;
+    v.main = dft2::dfttest_tc2_kernel<T, dft2::kFilterWiener, FMT, S>;
+    v.generic = dft2::dfttest_tc2_kernel<T, dft2::kFilterGeneric, FMT, S>;
     v.fixup = dft2::dfttest_fixup_kernel<16>;
     v.nw = 8;
     v.bpw = 2;
     v.minb = 2;
     return v;
 }
+template <int T, int FMT>
+Variant make_tc2_s(int S) {
+    switch (S) {
+    case 1: return make_tc2<T, FMT, 1>();
+    case 2: return make_tc2<T, FMT, 2>();
+    case 4: return make_tc2<T, FMT, 4>();
+    }
+    return Variant{};
+}
 }  // namespace
 
-Variant tc2_variant(int T, int fmt) {
-    if (T == 1) return fmt == dft2::kTc2Fp16 ? make_tc2<1, dft2::kTc2Fp16>() : make_tc2<1, dft2::kTc2Bf16>();
-    if (T == 3) return fmt == dft2::kTc2Fp16 ? make_tc2<3, dft2::kTc2Fp16>() : make_tc2<3, dft2::kTc2Bf16>();
+Variant tc2_variant(int T, int fmt, int S) {
+    if (T == 1) return fmt == dft2::kTc2Fp16 ? make_tc2_s<1, dft2::kTc2Fp16>(S) : make_tc2_s<1, dft2::kTc2Bf16>(S);
+    if (T == 3) return fmt == dft2::kTc2Fp16 ? make_tc2_s<3, dft2::kTc2Fp16>(S) : make_tc2_s<3, dft2::kTc2Bf16>(S);
     return Variant{};
 }
 
