@@ -368,6 +368,7 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
             int sc[4];  // source columns (mirror padding)
 #pragma unroll
             for (int i = 0; i < 4; ++i) sc[i] = mirror(min(x0 + g4 * 4 + i, pw - 1) - ox, W);
+            const bool fast4 = sc[3] == sc[0] + 3 && ((sc[0] - xa) & 3) == 0;
             float pv[NP][4];
 #pragma unroll
             for (int p = 0; p < NP; ++p)
@@ -379,8 +380,16 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
                 float xv[4];
                 if (staged) {
                     const unsigned char* srow = s_stg + ((slot * T + t) * S + r) * srb;
+                    if (fast4) {  // four in-plane samples, aligned in the staged row: one vector load
+                        const float4 q4 = stage_load4(srow, sc[0] - xa, P.kind);
+                        xv[0] = q4.x;
+                        xv[1] = q4.y;
+                        xv[2] = q4.z;
+                        xv[3] = q4.w;
+                    } else {
 #pragma unroll
-                    for (int i = 0; i < 4; ++i) xv[i] = stage_load1(srow, sc[i] - xa, P.kind);
+                        for (int i = 0; i < 4; ++i) xv[i] = stage_load1(srow, sc[i] - xa, P.kind);
+                    }
                 } else {
 #pragma unroll
                     for (int i = 0; i < 4; ++i) xv[i] = load_sample(job.src[t], rowoff + sc[i], P.kind);
@@ -450,6 +459,7 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
                     const uint32_t dc = tmem + lane_base + C_X + (2 * hf) * NJ;
                     const uint32_t ds = dc + NJ;
                     float g = 0.0f;
+                    const int zm_mask = P.g_div != 0.0f ? hd.wmask : 0;  // temporal bins with zero-mean terms
 #pragma unroll
                     for (int pass = 0; pass < 2; ++pass) {
                         float vc[NP][8], vs[NP][8];
@@ -501,18 +511,32 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
                                 kr[2] = zr[1] + zi[2];
                                 ki[2] = zi[1] - zr[2];
                             }
+                            // per temporal bin: U = Z - g W, m = gain(|U|^2, sigma), sum of m U over the bins,
+                            // plus g times the sum of W (the add-back of the zero-mean terms, summed once);
+                            // bins whose window spectrum is zero skip the subtraction
                             float sr = 0.0f, si = 0.0f;
+                            float4 tb0;
 #pragma unroll
                             for (int kt = 0; kt < T; ++kt) {
                                 const float4 tb = c_tab[(kt * 9 + ky) * 16 + kx];
-                                float re = kr[kt], im = ki[kt];
-                                // temporal bins whose window spectrum is zero skip the zero-mean terms
-                                if ((hd.wmask >> kt) & 1)
-                                    apply_bin<FC, true>(re, im, tb.x, tb.x, false, make_float2(tb.y, tb.z), g, P);
-                                else
-                                    apply_bin<FC, false>(re, im, tb.x, tb.x, false, make_float2(0.f, 0.f), 0.f, P);
-                                sr += re;
-                                si += im;
+                                if (kt == 0) tb0 = tb;
+                                float dre = kr[kt], dim = ki[kt];
+                                if (zm_mask & (1 << kt)) {
+                                    dre = fmaf(-g, tb.y, dre);
+                                    dim = fmaf(-g, tb.z, dim);
+                                }
+                                const float psd = fmaf(dim, dim, dre * dre);
+                                const float m =
+                                    FC == kFilterWiener ? gain<0>(psd, tb.x, P) : gain_rt(P.filter_type, psd, tb.x, P);
+                                sr = fmaf(m, dre, sr);
+                                si = fmaf(m, dim, si);
+                            }
+                            if (zm_mask) {
+                                // sum over the bins of W: in the w slots of bins 0 and 1 (T = 3), W itself (T = 1)
+                                const float swr = T == 1 ? tb0.y : tb0.w;
+                                const float swi = T == 1 ? tb0.z : c_tab[(9 + ky) * 16 + kx].w;
+                                sr = fmaf(g, swr, sr);
+                                si = fmaf(g, swi, si);
                             }
                             if (active) s_z[(b * 9 + ky) * kTc2ZPitch + kx] = make_float2(sr, si);
                         }

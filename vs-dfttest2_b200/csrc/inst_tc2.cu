@@ -191,6 +191,20 @@ int tc2_build(const Tc2Input& in, std::vector<char>& img, Tc2Shape& shape, std::
             const float* e = reinterpret_cast<const float*>(&img[h.off_tab]) + 4 * (kt * 9 * 16 + i);
             if (e[1] != 0.0f || e[2] != 0.0f) h.wmask |= 1 << kt;
         }
+    // sum over the temporal bins of the window spectrum of each (ky, kx): re in the w slot of bin 0,
+    // im in the w slot of bin 1 (the gain adds g times it back once)
+    if (T == 3) {
+        float* tab = reinterpret_cast<float*>(&img[h.off_tab]);
+        for (int i = 0; i < 9 * 16; ++i) {
+            double sre = 0.0, sim = 0.0;
+            for (int kt = 0; kt < T; ++kt) {
+                sre += tab[4 * (kt * 9 * 16 + i) + 1];
+                sim += tab[4 * (kt * 9 * 16 + i) + 2];
+            }
+            tab[4 * i + 3] = (float)sre;
+            tab[4 * (9 * 16 + i) + 3] = (float)sim;
+        }
+    }
     std::memcpy(&img[0], &h, sizeof(h));
     shape.nbx = h.nbx;
     shape.xg = h.xg;
