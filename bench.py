@@ -437,6 +437,33 @@ def autograd_measure(steps=10, warmup=3):
                         "(3,16,9) = 0.05, MSE to clean; forward vs forward + backward (adjoint kernel)"}
 
 
+def strip_form_flops(planes_hw, frames, B=16, S=4, T=3):
+    """Tensor-core FLOPs (2 M N K per MMA, as issued: padded rows and the
+    Toeplitz columns included) of one launch of the strip form over `frames`
+    frames of planes of sizes `planes_hw`: per block row of a strip of up to
+    16 blocks, the y products (T planes x 3 split products, 128 x 16 x 16),
+    the x products (per 8-block tile, cos and sin parts, ceil((16 + 7 S) / 16)
+    K steps x 3, 128 x 16T x 16) and the inverse-y products (per tile, 3,
+    128 x 16 x 16)."""
+    def pad_num(n):
+        pad = n + ((B - n % B) if n % B else 0) + 2 * max(B - S, S)
+        return (pad - B) // S + 1
+
+    nks = (B + 7 * S + 15) // 16
+    per_mma = lambda n: 2 * 128 * n * 16
+    total = 0
+    for h, w in planes_hw:
+        pnx, pny = pad_num(w), pad_num(h)
+        nsx = (pnx + 15) // 16
+        tiles = 0
+        for sx in range(nsx):
+            nb = (sx + 1) * pnx // nsx - sx * pnx // nsx
+            tiles += 1 if nb <= 8 else 2
+        row = T * 3 * per_mma(16) * nsx + tiles * (2 * nks * 3 * per_mma(16 * T) + 3 * per_mma(16))
+        total += row * pny
+    return total * frames
+
+
 def reference_parity(args, host_planes, outs, frames, r):
     """Max LSB and exact-match fraction of device outputs against the
     reference's CPU math (oracle/_ref) on sampled output frames, all planes.
@@ -615,6 +642,15 @@ def main():
             tc_results[mode] = {"value": world * (hi - lo) / (ms_tc * 1e-3), "unit": "frames/s", "ms_per_step": ms_tc,
                                 "speedup_vs_fp32": ms_per_step / ms_tc, "max_lsb_vs_fp32": worst,
                                 "exact_vs_fp32": exact / max(total, 1), "steps": opts.tc_steps}
+            if mode in ("tc_fp16x3", "tc_bf16x3"):
+                # the strip form's tensor-core work against the measured dense 16-bit peak
+                fl = strip_form_flops([tuple(p.shape[1:]) for p in host_planes], hi - lo)
+                peak_tc = measured_peaks().get("bf16_tflops")
+                tc_results[mode]["tensor"] = {
+                    "tflop_per_step": fl / 1e12, "achieved_tflops": fl / (ms_tc * 1e-3) / 1e12,
+                    "peak_tflops": peak_tc, "frac": (fl / (ms_tc * 1e-3) / 1e12 / peak_tc) if peak_tc else None,
+                    "peak_source": measured_peaks().get("source") + ", bf16_tflops burst (fp16 runs at the same dense rate)",
+                    "note": "FLOPs as issued (2 M N K per tcgen05.mma, padded rows and Toeplitz columns included)"}
         flt.set_precision("fp32")
 
     # ---- end to end through the C ABI host path (pinned host buffers)
