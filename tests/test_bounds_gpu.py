@@ -6,7 +6,8 @@
   still hold the canary.  Odd plane sizes, every block size / temporal size,
   sample types u8 / u16 / f32, row offsets that defeat the vector stores and
   the TMA staging (and aligned ones that use them).  Outputs must equal a
-  run on dense planes bit for bit.
+  run on dense planes bit for bit.  The FP32 kernels and the tensor-core
+  strip form.
 * The checked build (libdfttest2_b200_checked.so, -DDFT_CHECKS): the unit
   and fix-up kernels test every ring, staging, block-buffer, band-record and
   output index before the access and record kernel error 3 instead; the same
@@ -79,13 +80,19 @@ def _run_guarded(flt, clip, st, bits, aligned, torch):
     return out, intact
 
 
-@pytest.mark.parametrize("B,sosize,tb", SHAPES)
-def test_guard_bands(B, sosize, tb, cuda_device):
+# the tensor-core strip form (16x16 blocks, block steps 1, 2, 4, radius 0 or 1)
+STRIP_SHAPES = [(16, 12, 3), (16, 14, 3), (16, 15, 1), (16, 12, 1)]
+
+
+@pytest.mark.parametrize("B,sosize,tb,precision", [s + ("fp32",) for s in SHAPES] +
+                         [s + ("tc_fp16x3",) for s in STRIP_SHAPES])
+def test_guard_bands(B, sosize, tb, precision, cuda_device):
     import torch
 
     args = plugin_arguments(ftype=0, sigma=6.0, sbsize=B, sosize=sosize, tbsize=tb)
     rng = np.random.default_rng(B * 100 + sosize * 10 + tb)
     flt = Filter(device_id=0, **args)
+    flt.set_precision(precision)
     try:
         for (w, h) in SIZES:
             for dtype, st, bits in KINDS:
@@ -96,7 +103,7 @@ def test_guard_bands(B, sosize, tb, cuda_device):
                 dense = dense.cpu().numpy().view(clip.dtype)
                 for aligned in (True, False):
                     out, intact = _run_guarded(flt, clip, st, bits, aligned, torch)
-                    what = f"B{B} sosize {sosize} T{tb} {w}x{h} {dtype.__name__} aligned {aligned}"
+                    what = f"B{B} sosize {sosize} T{tb} {precision} {w}x{h} {dtype.__name__} aligned {aligned}"
                     assert intact, f"guard bytes overwritten: {what}"
                     assert np.array_equal(out.view(np.uint8), dense.view(np.uint8)), f"{what}: differs from dense planes"
     finally:
