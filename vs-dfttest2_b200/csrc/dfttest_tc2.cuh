@@ -600,15 +600,16 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
                 }
                 const int x = quarter * 32 + lane;
                 constexpr int CPH = NJ / 2;  // columns per half
+                float v[CPH / 8][8];  // every load issued before one wait
 #pragma unroll
-                for (int c8 = 0; c8 < CPH / 8; ++c8) {
-                    const int n0 = hf * CPH + c8 * 8;
-                    float v[8];
-                    tmem_ld8(tmem + lane_base + C_Y + n0, v);
-                    tmem_wait_ld();
-                    if (x < XG * 8) {
+                for (int c8 = 0; c8 < CPH / 8; ++c8) tmem_ld8(tmem + lane_base + C_Y + hf * CPH + c8 * 8, v[c8]);
+                tmem_wait_ld();
+                if (x < XG * 8) {
+#pragma unroll
+                    for (int c8 = 0; c8 < CPH / 8; ++c8) {
+                        const int n0 = hf * CPH + c8 * 8;
                         char* dst = s_yb + (n0 / 8) * (XG * 128) + (x >> 3) * 128 + (x & 7) * 16;
-                        put_row8<FMT>(dst, dst + L.yb_hl, v);
+                        put_row8<FMT>(dst, dst + L.yb_hl, v[c8]);
                     }
                 }
             }
