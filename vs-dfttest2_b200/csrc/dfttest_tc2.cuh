@@ -724,12 +724,19 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
                         const int px = 4 * q;
                         const int b_lo = px + 4 <= 16 ? 0 : (px + 4 - 16 + S - 1) / S;
                         const int b_hi = min(px / S, nbx - 1);
-                        for (int b = b_lo; b <= b_hi; ++b) {
-                            const float4 w4 = *reinterpret_cast<const float4*>(row + b * 16 + (px - b * S));
-                            acc.x += w4.x;
-                            acc.y += w4.y;
-                            acc.z += w4.z;
-                            acc.w += w4.w;
+                        constexpr int NK = 16 / S;  // covering blocks at most: loads issued together
+                        float4 w4[NK];
+#pragma unroll
+                        for (int k = 0; k < NK; ++k)
+                            w4[k] = b_lo + k <= b_hi
+                                        ? *reinterpret_cast<const float4*>(row + (b_lo + k) * 16 + (px - (b_lo + k) * S))
+                                        : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                        for (int k = 0; k < NK; ++k) {  // ascending block order
+                            acc.x += w4[k].x;
+                            acc.y += w4[k].y;
+                            acc.z += w4[k].z;
+                            acc.w += w4[k].w;
                         }
                     } else {
 #pragma unroll
