@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
     char* c_wy = tc2_smem;
     char* c_wx = tc2_smem + (hd.off_wx - hd.off_wy);
     char* c_wi = tc2_smem + (hd.off_wi - hd.off_wy);
-    const float4* c_tab = reinterpret_cast<const float4*>(tc2_smem + (hd.off_tab - hd.off_wy));
+    const float4* __restrict__ c_tab = reinterpret_cast<const float4*>(tc2_smem + (hd.off_tab - hd.off_wy));
     char* s_ring = tc2_smem + L.ring;
     char* s_yb = tc2_smem + L.yb;
     float2* s_z = reinterpret_cast<float2*>(tc2_smem + L.yb);  // gain output, aliases the Y operand
@@ -482,7 +482,9 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
                             const float dc0 = __shfl_sync(0xffffffffu, vc[0][0], lane & 16);
                             g = P.g_div != 0.0f ? __fdiv_rn(dc0, P.g_div) : 0.0f;
                         }
-                        // y-bins of this pass: pass 0 -> 0, 1, 2, 3; pass 1 -> 4, 5, 6, 7, 8
+                        // y-bins of this pass: pass 0 -> 0, 1, 2, 3; pass 1 -> 4, 5, 6, 7, 8; their outputs are
+                        // stored after the pass, so that no store sits between the table loads of the bins
+                        float2 outv[5];
 #pragma unroll
                         for (int kk = 0; kk < 5; ++kk) {
                             if (pass == 0 && kk == 4) continue;
@@ -538,7 +540,14 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
                                 sr = fmaf(g, swr, sr);
                                 si = fmaf(g, swi, si);
                             }
-                            if (active) s_z[(b * 9 + ky) * kTc2ZPitch + kx] = make_float2(sr, si);
+                            outv[kk] = make_float2(sr, si);
+                        }
+                        if (active) {
+#pragma unroll
+                            for (int kk = 0; kk < 5; ++kk) {
+                                if (pass == 0 && kk == 4) continue;
+                                s_z[(b * 9 + (pass == 0 ? kk : 4 + kk)) * kTc2ZPitch + kx] = outv[kk];
+                            }
                         }
                     }
                 }
@@ -753,9 +762,26 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
                         store4(job.dst, (long long)(py - oy) * job.dst_stride + (gx - ox), acc, P.kind, P.peak,
                                inv_scale);
                     } else {
+                        // a segment of the unit's band (shared with a neighbour): one vector store into the
+                        // band record when its 4 pixels are in the plane and contiguous there, else per pixel
+                        bool done = false;
+                        if (4 * q + 4 <= u.fw && gx >= ox && gx + 4 <= ox + W && py >= oy && py < oy + Hh &&
+                            !(py >= excl_y0 && py < excl_y1 && gx + 3 >= excl_x0 && gx < excl_x1)) {
+                            const int ly = py - u.by0 * S;
+                            const int i0 = band_index(4 * q, ly, u.fw, u.fh, O);
+                            const int i3 = band_index(4 * q + 3, ly, u.fw, u.fh, O);
+                            float* dst = rec + i0;
+                            if (i3 == i0 + 3 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0 &&
+                                DFT_IN_RANGE(i3, a.rec_stride, a.error_flag)) {
+                                *reinterpret_cast<float4*>(dst) = acc;
+                                done = true;
+                            }
+                        }
+                        if (!done) {
 #pragma unroll
-                        for (int i = 0; i < 4; ++i)
-                            if (4 * q + i < u.fw) finish_px(fg, py, 4 * q + i, av[i]);
+                            for (int i = 0; i < 4; ++i)
+                                if (4 * q + i < u.fw) finish_px(fg, py, 4 * q + i, av[i]);
+                        }
                     }
                 }
             }
