@@ -150,22 +150,42 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float (&v)[16]) {
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15, %16};" ::"r"(taddr),
-        "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3])),
-        "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])), "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])),
-        "r"(__float_as_uint(v[8])), "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])),
-        "r"(__float_as_uint(v[11])), "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])),
-        "r"(__float_as_uint(v[14])), "r"(__float_as_uint(v[15]))
-        : "memory");
-}
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
-// packed real-DFT bin index of y-bin ky: j 0 = Re 0, 1 = Re 8, 2k = Re k, 2k + 1 = Im k
-__host__ __device__ constexpr int tc2_jre(int ky) { return ky == 0 ? 0 : (ky == 8 ? 1 : 2 * ky); }
-__host__ __device__ constexpr int tc2_jim(int ky) { return 2 * ky + 1; }
+// N (1, 2 or 4) consecutive 32-bit columns of this thread's lane: load, store
+template <int N> __device__ __forceinline__ void tmem_ld_n(uint32_t taddr, float (&v)[N]) {
+    uint32_t r[4];
+    if constexpr (N == 1) {
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r[0]) : "r"(taddr));
+    } else if constexpr (N == 2) {
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(taddr));
+    } else {
+        static_assert(N == 4, "1, 2 or 4 columns");
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                     : "r"(taddr));
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i) v[i] = __uint_as_float(r[i]);
+}
+template <int N> __device__ __forceinline__ void tmem_st_n(uint32_t taddr, const uint32_t (&v)[N]) {
+    if constexpr (N == 1) {
+        asm volatile("tcgen05.st.sync.aligned.32x32b.x1.b32 [%0], {%1};" ::"r"(taddr), "r"(v[0]) : "memory");
+    } else if constexpr (N == 2) {
+        asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};" ::"r"(taddr), "r"(v[0]), "r"(v[1])
+                     : "memory");
+    } else {
+        static_assert(N == 4, "1, 2 or 4 columns");
+        asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), "r"(v[0]),
+                     "r"(v[1]), "r"(v[2]), "r"(v[3])
+                     : "memory");
+    }
+}
+
+// packed real-DFT bin index of y-bin ky: j 0 = Re 0, (1, 2) = (Re, Im) 1, (3, 4) = 2, (5, 6) = 3,
+// 7 = Re 8, (8, 9) = (Re, Im) 4, ..., (14, 15) = 7: y-bins 0, 1, 2, 3, 8 in j 0..7, 4..7 in j 8..15
+__host__ __device__ constexpr int tc2_jre(int ky) { return ky == 0 ? 0 : (ky == 8 ? 7 : (ky <= 3 ? 2 * ky - 1 : 2 * ky)); }
+__host__ __device__ constexpr int tc2_jim(int ky) { return ky <= 3 ? 2 * ky : 2 * ky + 1; }
 
 template <int T, int FC, int FMT, int SS>
 __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_constant__ KernelArgs a) {
@@ -468,36 +488,27 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
                             tmem_ld8(dc + 16 * p + 8 * pass, vc[p]);
                             tmem_ld8(ds + 16 * p + 8 * pass, vs[p]);
                         }
-                        float re8c[NP], re8s[NP];  // Re of y-bin 8 (j = 1) is in pass 0's columns
-                        if (pass == 1) {
-#pragma unroll
-                            for (int p = 0; p < NP; ++p) {
-                                tmem_ld1(dc + 16 * p + 1, re8c[p]);
-                                tmem_ld1(ds + 16 * p + 1, re8s[p]);
-                            }
-                        }
                         tmem_wait_ld();
                         if (pass == 0) {
                             // zero-mean: g = Re Z(0,0,0) / Re W(0,0,0), Z(0,0,0) held by lane kx = 0 of the block
                             const float dc0 = __shfl_sync(0xffffffffu, vc[0][0], lane & 16);
                             g = P.g_div != 0.0f ? __fdiv_rn(dc0, P.g_div) : 0.0f;
                         }
-                        // y-bins of this pass: pass 0 -> 0, 1, 2, 3; pass 1 -> 4, 5, 6, 7, 8; their outputs are
-                        // stored after the pass, so that no store sits between the table loads of the bins
+                        // y-bins of this pass (their packed bins j lie in its 8 columns): pass 0 -> 0, 1, 2, 3, 8;
+                        // pass 1 -> 4, 5, 6, 7; outputs are stored after the pass, so that no store sits
+                        // between the table loads of the bins
                         float2 outv[5];
 #pragma unroll
                         for (int kk = 0; kk < 5; ++kk) {
-                            if (pass == 0 && kk == 4) continue;
-                            const int ky = pass == 0 ? kk : 4 + kk;
+                            if (pass == 1 && kk == 4) continue;
+                            const int ky = pass == 0 ? (kk == 4 ? 8 : kk) : 4 + kk;
                             float zr[NP], zi[NP];
 #pragma unroll
                             for (int p = 0; p < NP; ++p) {
-                                if (ky == 0) {
-                                    zr[p] = vc[p][0];
-                                    zi[p] = -vs[p][0];
-                                } else if (ky == 8) {
-                                    zr[p] = re8c[p];
-                                    zi[p] = -re8s[p];
+                                if (ky == 0 || ky == 8) {  // real in y: no imaginary column
+                                    const int jr = tc2_jre(ky) - 8 * pass;
+                                    zr[p] = vc[p][jr];
+                                    zi[p] = -vs[p][jr];
                                 } else {
                                     const int jr = tc2_jre(ky) - 8 * pass, ji = tc2_jim(ky) - 8 * pass;
                                     zr[p] = vc[p][jr] + vs[p][ji];
@@ -545,8 +556,8 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
                         if (active) {
 #pragma unroll
                             for (int kk = 0; kk < 5; ++kk) {
-                                if (pass == 0 && kk == 4) continue;
-                                s_z[(b * 9 + (pass == 0 ? kk : 4 + kk)) * kTc2ZPitch + kx] = outv[kk];
+                                if (pass == 1 && kk == 4) continue;
+                                s_z[(b * 9 + (pass == 0 ? (kk == 4 ? 8 : kk) : 4 + kk)) * kTc2ZPitch + kx] = outv[kk];
                             }
                         }
                     }
@@ -675,22 +686,30 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
                     const int blk = l >> 4, x = l & 15;
                     const int b = hf * 8 + blk;
                     const uint32_t col = tmem + lane_base + C_OUT + 16 * hf;
-                    float v[16];
-                    tmem_ld16(col, v);
-                    tmem_wait_ld();
-                    if (hf < ntile && b < nbx) {
-                        const float w = hd.sx[x];
+                    const bool mine = hf < ntile && b < nbx;
+                    const float w = hd.sx[x];
+                    if (last) {
+                        float v[16];
+                        tmem_ld16(col, v);
+                        tmem_wait_ld();
+                        if (mine) {
 #pragma unroll
-                        for (int y = 0; y < 16; ++y) {  // column y holds output row bb S + ((y - c0) mod 16)
-                            const int r = (y - c0) & 15;
-                            if (last || r < S) s_fin[(r * 16 + b) * 16 + x] = v[y] * w;
+                            for (int y = 0; y < 16; ++y)  // column y holds output row bb S + ((y - c0) mod 16)
+                                s_fin[((((y - c0) & 15)) * 16 + b) * 16 + x] = v[y] * w;
                         }
-                    }
-                    if (!last) {
+                    } else {
+                        // the S columns c0 .. c0 + S - 1 (c0 + S <= 16): read, then restart from zero
+                        float v[S];
+                        uint32_t z[S];
+                        tmem_ld_n<S>(col + c0, v);
+                        tmem_wait_ld();
 #pragma unroll
-                        for (int y = 0; y < 16; ++y)
-                            if (((y - c0) & 15) < S) v[y] = 0.0f;
-                        tmem_st16(col, v);
+                        for (int r = 0; r < S; ++r) z[r] = 0u;
+                        tmem_st_n<S>(col + c0, z);
+                        if (mine) {
+#pragma unroll
+                            for (int r = 0; r < S; ++r) s_fin[(r * 16 + b) * 16 + x] = v[r] * w;
+                        }
                         tmem_wait_st();
                     }
                 }
