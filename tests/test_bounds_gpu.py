@@ -10,9 +10,10 @@
   strip form.
 * The checked build (libdfttest2_b200_checked.so, -DDFT_CHECKS): the unit
   and fix-up kernels test every ring, staging, block-buffer, band-record and
-  output index before the access and record kernel error 3 instead; the same
-  cases run through it in a child process (the library is chosen at load
-  time) and dfttest2_b200_check must report nothing.
+  output index before the access, the strip form its band-record indices,
+  and a failing test records kernel error 3 instead of the access; the same
+  cases (both forms) run through it in a child process (the library is
+  chosen at load time) and dfttest2_b200_check must report nothing.
 """
 import os
 import subprocess
@@ -121,9 +122,10 @@ from dfttest2_b200.plugin import Filter
 from oracle import oracle as O
 rng = np.random.default_rng(3)
 worst = 0
-for B, sosize, tb in {shapes!r}:
+for B, sosize, tb, precision in {shapes!r}:
     args = plugin_arguments(ftype=0, sigma=6.0, sbsize=B, sosize=sosize, tbsize=tb)
     flt = Filter(device_id=0, **args)
+    flt.set_precision(precision)
     for (w, h) in {sizes!r}:
         x = np.round(np.clip(0.5 + 0.2 * rng.standard_normal((3, h, w)), 0, 1) * 65535).astype(np.uint16)
         out = flt.process_clip_device(torch.from_numpy(x.view(np.int16)).cuda(), 0, 16)
@@ -144,7 +146,8 @@ def test_checked_build_reports_no_out_of_range_index(cuda_device):
     lib = os.path.join(pkg, "dfttest2_b200", "libdfttest2_b200_checked.so")
     if not os.path.exists(lib):
         pytest.fail("the checked build is missing: run `make checked` in vs-dfttest2_b200/")
-    code = CHILD.format(root=root, pkg=pkg, shapes=SHAPES, sizes=SIZES)
+    shapes = [s + ("fp32",) for s in SHAPES] + [s + ("tc_fp16x3",) for s in STRIP_SHAPES]
+    code = CHILD.format(root=root, pkg=pkg, shapes=shapes, sizes=SIZES)
     env = dict(os.environ, DFTTEST2_B200_LIB="checked")
     res = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
     print(res.stdout[-2000:], res.stderr[-2000:])
