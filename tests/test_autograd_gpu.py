@@ -34,15 +34,17 @@ def _reference_grads(torch, args, noisy, clean, sigma, device):
 
 @pytest.mark.parametrize("kw", [dict(ftype=0, sigma=3.0, tbsize=3), dict(ftype=0, sigma=2.0, tbsize=1),
                                 dict(ftype=4, sigma=1.1, pmin=2.0, pmax=300.0, tbsize=3),
-                                dict(ftype=0, f0beta=0.7, sigma=3.0, tbsize=5, swin=2)])
+                                dict(ftype=0, f0beta=0.7, sigma=3.0, tbsize=5, swin=2),
+                                dict(ftype=0, sigma=3.0, tbsize=3, sbsize=8, sosize=4),
+                                dict(ftype=0, sigma=3.0, tbsize=3, sbsize=32, sosize=16)])
 def test_gradients_match_fp64_reference(kw, cuda_device):
     import torch
 
     from dfttest2_b200.autograd import DFTTestModule
 
     args, noisy, clean = _setup(torch, **kw)
-    T = 2 * args["radius"] + 1
-    sigma0 = torch.tensor(args["sigma"], dtype=torch.float32).reshape(T, 16, 9)
+    T, B = 2 * args["radius"] + 1, args["block_size"]
+    sigma0 = torch.tensor(args["sigma"], dtype=torch.float32).reshape(T, B, B // 2 + 1)
     mod = DFTTestModule(args, sigma0, device=cuda_device)
     x = noisy.to(cuda_device).requires_grad_(True)
     out = mod(x)

@@ -18,8 +18,9 @@
 //   dx += scale * w .* dz                    (transposed gather, through the mirror)
 // Block spectra are recomputed from the input, not stored by the forward.
 // A CTA takes a tile of neighbouring blocks at a time (persistent grid over
-// tiles); the sigma gradient stays in registers across tiles and is reduced
-// once per CTA.
+// tiles); the sigma gradient is summed in shared memory across the tiles and
+// added to global memory once per CTA.  DFT_t, the gain adjoint and IDFT_t
+// run in one pass, in registers, per (ky, kx) bin.
 #pragma once
 
 #include "dfttest_kernel.cuh"
@@ -166,11 +167,13 @@ struct AdjTile {
     static constexpr int NTH = WIDE ? 384 : 256;
     static constexpr int GT = NTH / NBLK;              // threads per block in the gain phase
     static_assert(NTH % NBLK == 0 && (GT & (GT - 1)) == 0, "the zero-mean reduction shuffles over a power of two");
-    static constexpr int NPER = (SPEC + GT - 1) / GT;  // gain bins per thread
+    static constexpr int NPER = (B * X + GT - 1) / GT;  // (ky, kx) bins per thread in the gain phase
     // shared memory (floats), in order
-    static constexpr int o_win = 0;                    // scale * window   [T][B][B]
-    static constexpr int o_wsyn = o_win + T * B * B;   // wsyn / scale     [B][B]
-    static constexpr int o_sig = o_wsyn + B * B;       // sigma            [SPEC]
+    // window rows WP = B + 1 floats apart: the row tasks of a warp differ in y and read the same x
+    static constexpr int WP = B + 1;
+    static constexpr int o_win = 0;                    // scale * window   [T][B][WP]
+    static constexpr int o_wsyn = o_win + T * B * WP;  // wsyn / scale     [B][WP]
+    static constexpr int o_sig = o_wsyn + B * WP;      // sigma            [SPEC]
     static constexpr int o_wf = o_sig + SPEC;          // window spectrum  [SPEC][2]
     static constexpr int o_tw = o_wf + 2 * SPEC;       // conj temporal twiddles [T][2]
     static constexpr int o_dg = o_tw + 2 * T;          // zero-mean partials [NBLK]
@@ -210,7 +213,7 @@ template <int B, int T>
 __global__ void __launch_bounds__(AdjTile<B, T>::NTH, 2) dfttest_adjoint_kernel(const __grid_constant__ AdjointArgs a) {
     using L = AdjTile<B, T>;
     constexpr int X = L::X, SPEC = L::SPEC, NBLK = L::NBLK, TBX = L::TBX, TBY = L::TBY, GT = L::GT;
-    constexpr int TS = L::TS, ZB = L::ZB;
+    constexpr int TS = L::TS, ZB = L::ZB, WP = L::WP;
     constexpr int R = (T - 1) / 2;
     extern __shared__ __align__(16) float smem[];
     float* s_win = smem + L::o_win;
@@ -227,8 +230,8 @@ __global__ void __launch_bounds__(AdjTile<B, T>::NTH, 2) dfttest_adjoint_kernel(
     const int tid = threadIdx.x;
     const int S = a.block_step, PH = a.patch_h, PW = a.patch_w, PP = L::patch_pitch(a.patch_w);
 
-    for (int i = tid; i < T * B * B; i += L::NTH) s_win[i] = a.scale * a.win[i];
-    for (int i = tid; i < B * B; i += L::NTH) s_wsyn[i] = a.wsyn[i] / a.scale;
+    for (int i = tid; i < T * B * B; i += L::NTH) s_win[(i / B) * WP + i % B] = a.scale * a.win[i];
+    for (int i = tid; i < B * B; i += L::NTH) s_wsyn[(i / B) * WP + i % B] = a.wsyn[i] / a.scale;
     for (int i = tid; i < SPEC; i += L::NTH) {
         s_sig[i] = a.sigma[i];
         s_wf[2 * i] = a.zero_mean ? a.wf[2 * i] : 0.0f;
@@ -290,7 +293,7 @@ __global__ void __launch_bounds__(AdjTile<B, T>::NTH, 2) dfttest_adjoint_kernel(
                 if (valid) {
                     const float* row = dxp + (t * PH + (blk / TBX) * S + y) * PP + (blk % TBX) * S;
 #pragma unroll
-                    for (int x = 0; x < B; ++x) v[x] = s_win[(t * B + y) * B + x] * row[x];
+                    for (int x = 0; x < B; ++x) v[x] = s_win[(t * B + y) * WP + x] * row[x];
                 } else {
 #pragma unroll
                     for (int x = 0; x < B; ++x) v[x] = 0.0f;
@@ -303,7 +306,7 @@ __global__ void __launch_bounds__(AdjTile<B, T>::NTH, 2) dfttest_adjoint_kernel(
 #pragma unroll
                 for (int x = 0; x < B; ++x) {
                     const int px = px0 + x;
-                    v[x] = rin && px >= ox && px < ox + W ? __ldg(row + px - ox) * s_wsyn[y * B + x] : 0.0f;
+                    v[x] = rin && px >= ox && px < ox + W ? __ldg(row + px - ox) * s_wsyn[y * WP + x] : 0.0f;
                 }
                 r2c_n<B>(v, o);
                 float* dr = gr + blk * B * X + y * X;
@@ -339,59 +342,63 @@ __global__ void __launch_bounds__(AdjTile<B, T>::NTH, 2) dfttest_adjoint_kernel(
                 pi[y * X] = im[y];
             }
         }
-        if constexpr (T > 1) {
-            __syncthreads();
-            for (int task = tid; task < NBLK * B * X; task += L::NTH) {  // DFT_t of every (ky, kx)
-                const int blk = task / (B * X), bin = task - blk * (B * X);
-                float* pr = zr + blk * ZB + bin;
-                float* pi = zi + blk * ZB + bin;
-                float re[T], im[T];
-#pragma unroll
-                for (int t = 0; t < T; ++t) {
-                    re[t] = pr[t * TS];
-                    im[t] = pi[t * TS];
-                }
-                cdft_n<T>(re, im, false);
-#pragma unroll
-                for (int t = 0; t < T; ++t) {
-                    pr[t * TS] = re[t];
-                    pi[t * TS] = im[t];
-                }
-            }
-        }
         __syncthreads();
 
-        // ---- through the gain and the zero-mean offset; thread owns bins gj + k GT of block gblk
+        // ---- per (ky, kx) bin: DFT_t, the gain and its adjoint, the inverse DFT_t, in registers;
+        //      thread owns bins gj + k GT of block gblk (every temporal bin of each)
         {
+            constexpr int BX = B * X;
             float* br = zr + gblk * ZB;
             float* bi = zi + gblk * ZB;
             const float* cr = gr + gblk * B * X;
             const float* ci = gi + gblk * B * X;
-            const float g = a.zero_mean ? br[0] / wf0 : 0.0f;
+            // g = Re Z(0) / Re WF(0), Z(0) = the sum over the frames of bin (0, 0)
+            float g = 0.0f;
+            if (a.zero_mean) {
+#pragma unroll
+                for (int t = 0; t < T; ++t) g += br[t * TS];
+                g /= wf0;
+            }
             float dg = 0.0f;
             // the filter type is uniform: one switch around the bins keeps the executed code one straight run
             auto bins = [&](auto ftc) {
                 constexpr int FT = decltype(ftc)::value;
 #pragma unroll
                 for (int k = 0; k < L::NPER; ++k) {
-                    const int i = gj + k * GT;
-                    if (SPEC % GT == 0 || i < SPEC) {
-                        const int kt = i / (B * X), bin = i - kt * (B * X);
-                        const int zi_ = kt * TS + bin;  // index in the padded spectra
-                        const float cs = s_tw[2 * kt], sn = s_tw[2 * kt + 1];
-                        const float Gr = cr[bin] * cs - ci[bin] * sn;
-                        const float Gi = cr[bin] * sn + ci[bin] * cs;
-                        const float wr = s_wf[2 * i], wi = s_wf[2 * i + 1];
-                        const float dr = br[zi_] - g * wr, di = bi[zi_] - g * wi;
-                        float m, dpsd, dsig;
-                        gain_grad<FT>(dr * dr + di * di, s_sig[i], a, m, dpsd, dsig);
-                        const float q = Gr * dr + Gi * di;
-                        const float ddr = m * Gr + 2.0f * dpsd * q * dr;
-                        const float ddi = m * Gi + 2.0f * dpsd * q * di;
-                        if (a.gsigma && dsig != 0.0f) atomicAdd(&s_gs[i], dsig * q);
-                        dg += (Gr * wr + Gi * wi) - (ddr * wr + ddi * wi);
-                        br[zi_] = ddr;
-                        bi[zi_] = ddi;
+                    const int bin = gj + k * GT;
+                    if (BX % GT == 0 || bin < BX) {
+                        float re[T], im[T];
+#pragma unroll
+                        for (int t = 0; t < T; ++t) {
+                            re[t] = br[t * TS + bin];
+                            im[t] = bi[t * TS + bin];
+                        }
+                        if constexpr (T > 1) cdft_n<T>(re, im, false);
+                        const float hr = cr[bin], hi = ci[bin];
+#pragma unroll
+                        for (int kt = 0; kt < T; ++kt) {
+                            const int i = kt * BX + bin;
+                            const float cs = s_tw[2 * kt], sn = s_tw[2 * kt + 1];
+                            const float Gr = hr * cs - hi * sn;
+                            const float Gi = hr * sn + hi * cs;
+                            const float wr = s_wf[2 * i], wi = s_wf[2 * i + 1];
+                            const float dr = re[kt] - g * wr, di = im[kt] - g * wi;
+                            float m, dpsd, dsig;
+                            gain_grad<FT>(dr * dr + di * di, s_sig[i], a, m, dpsd, dsig);
+                            const float q = Gr * dr + Gi * di;
+                            const float ddr = m * Gr + 2.0f * dpsd * q * dr;
+                            const float ddi = m * Gi + 2.0f * dpsd * q * di;
+                            if (a.gsigma && dsig != 0.0f) atomicAdd(&s_gs[i], dsig * q);
+                            dg += (Gr * wr + Gi * wi) - (ddr * wr + ddi * wi);
+                            re[kt] = ddr;
+                            im[kt] = ddi;
+                        }
+                        if constexpr (T > 1) cdft_n<T>(re, im, true);
+#pragma unroll
+                        for (int t = 0; t < T; ++t) {
+                            br[t * TS + bin] = re[t];
+                            bi[t * TS + bin] = im[t];
+                        }
                     }
                 }
             };
@@ -410,30 +417,10 @@ __global__ void __launch_bounds__(AdjTile<B, T>::NTH, 2) dfttest_adjoint_kernel(
             if ((tid & (RW - 1)) == 0) atomicAdd(&s_dg[gblk], dg);
         }
         __syncthreads();
-        if (a.zero_mean && tid < NBLK) zr[tid * ZB] += s_dg[tid] / wf0;
 
-        // ---- adjoint of the forward transform: inverse over t and y, halved c2r over x
-        if constexpr (T > 1) {
-            __syncthreads();
-            for (int task = tid; task < NBLK * B * X; task += L::NTH) {
-                const int blk = task / (B * X), bin = task - blk * (B * X);
-                float* pr = zr + blk * ZB + bin;
-                float* pi = zi + blk * ZB + bin;
-                float re[T], im[T];
-#pragma unroll
-                for (int t = 0; t < T; ++t) {
-                    re[t] = pr[t * TS];
-                    im[t] = pi[t * TS];
-                }
-                cdft_n<T>(re, im, true);
-#pragma unroll
-                for (int t = 0; t < T; ++t) {
-                    pr[t * TS] = re[t];
-                    pi[t * TS] = im[t];
-                }
-            }
-        }
-        __syncthreads();
+        // ---- adjoint of the forward transform: inverse over y, halved c2r over x (the inverse
+        //      over t ran with the gain).  The zero-mean term dg / Re WF(0) of bin (0, 0, 0) is, after
+        //      the inverse DFT_t, the same constant on bin (ky 0, kx 0) of every frame.
         for (int task = tid; task < NBLK * T * X; task += L::NTH) {
             const int blk = task / (T * X), rem = task - blk * (T * X);
             const int t = rem / X, kx = rem - t * X;
@@ -445,6 +432,7 @@ __global__ void __launch_bounds__(AdjTile<B, T>::NTH, 2) dfttest_adjoint_kernel(
                 re[y] = pr[y * X];
                 im[y] = pi[y * X];
             }
+            if (a.zero_mean && kx == 0) re[0] += s_dg[blk] / wf0;
             cdft_n<B>(re, im, true);
 #pragma unroll
             for (int y = 0; y < B; ++y) {
@@ -469,7 +457,7 @@ __global__ void __launch_bounds__(AdjTile<B, T>::NTH, 2) dfttest_adjoint_kernel(
             c2r_n<B>(v, o);
             float* dst = dxp + (t * PH + (blk / TBX) * S + y) * PP + (blk % TBX) * S;
 #pragma unroll
-            for (int x = 0; x < B; ++x) atomicAdd(dst + x, s_win[(t * B + y) * B + x] * o[x]);
+            for (int x = 0; x < B; ++x) atomicAdd(dst + x, s_win[(t * B + y) * WP + x] * o[x]);
         }
         __syncthreads();
 
