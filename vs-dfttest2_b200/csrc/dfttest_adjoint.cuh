@@ -62,12 +62,14 @@ __device__ __forceinline__ void gain_grad(float psd, float s, const AdjointArgs&
     dpsd = 0.0f;
     dsig = 0.0f;
     if constexpr (FT == 0) {
-        const float den = psd + eps;
-        const float u = (psd - s) / den;
+        // one MUFU reciprocal (< 1 ulp, as the forward kernel's Wiener gain) for the quotient and
+        // both derivatives
+        const float r = rcp_approx(psd + eps);
+        const float u = (psd - s) * r;
         m = fmaxf(u, 0.0f);
         if (u > 0.0f) {
-            dpsd = (s + eps) / (den * den);
-            dsig = -1.0f / den;
+            dpsd = (s + eps) * r * r;
+            dsig = -r;
         }
     } else if constexpr (FT == 1) {
         m = psd < s ? 0.0f : 1.0f;
@@ -80,13 +82,14 @@ __device__ __forceinline__ void gain_grad(float psd, float s, const AdjointArgs&
         dsig = in ? 1.0f : 0.0f;
     } else if constexpr (FT == 4) {
         const float D = (psd + a.pmin) * (psd + a.pmax) + eps;
-        const float h = psd * a.pmax / D;
+        const float rD = rcp_approx(D);
+        const float h = psd * a.pmax * rD;
         const float sh = sqrtf(h);
         m = s * sh;
         dsig = sh;
         if (h > 0.0f) {
-            const float dh = a.pmax / D - psd * a.pmax * (2.0f * psd + a.pmin + a.pmax) / (D * D);
-            dpsd = s * dh / (2.0f * sh);
+            const float dh = a.pmax * rD - psd * a.pmax * (2.0f * psd + a.pmin + a.pmax) * rD * rD;
+            dpsd = 0.5f * s * dh * rcp_approx(sh);
         }
     } else {  // 5: u^pmin, 6: sqrt(u)
         const float den = psd + eps;
@@ -176,6 +179,7 @@ struct AdjTile {
     static constexpr int o_sig = o_wsyn + B * WP;      // sigma            [SPEC]
     static constexpr int o_wf = o_sig + SPEC;          // window spectrum  [SPEC][2]
     static constexpr int o_tw = o_wf + 2 * SPEC;       // conj temporal twiddles [T][2]
+    static_assert(o_wf % 2 == 0, "the window spectrum is read as float2");
     static constexpr int o_dg = o_tw + 2 * T;          // zero-mean partials [NBLK]
     static constexpr int o_gs = o_dg + NBLK;           // sigma-gradient partials of the CTA [SPEC]
     // spectra [NBLK][T][B][X]: temporal planes TS floats apart, TS = X (mod
@@ -251,13 +255,18 @@ __global__ void __launch_bounds__(AdjTile<B, T>::NTH, 2) dfttest_adjoint_kernel(
     float* s_gs = smem + L::o_gs;
     for (int i = tid; i < SPEC; i += L::NTH) s_gs[i] = 0.0f;
 
+    const int lane = tid & 31, warp = tid >> 5;
+    int jn = 0;  // job of the current tile: a CTA visits its tiles in increasing order
     for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
-        int lo = 0, hi = a.njobs - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (a.jobs[mid].tile_base <= tile) lo = mid; else hi = mid - 1;
+        if (jn + 1 < a.njobs && a.jobs[jn + 1].tile_base <= tile) {
+            int lo = jn + 1, hi = a.njobs - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (a.jobs[mid].tile_base <= tile) lo = mid; else hi = mid - 1;
+            }
+            jn = lo;
         }
-        const GradJob& job = a.jobs[lo];
+        const GradJob& job = a.jobs[jn];
         const int W = job.width, Hh = job.height;
         const int pw = pad_size(W, B, S), ph = pad_size(Hh, B, S);
         const int pnx = (pw - B) / S + 1, pny = (ph - B) / S + 1;
@@ -267,17 +276,27 @@ __global__ void __launch_bounds__(AdjTile<B, T>::NTH, 2) dfttest_adjoint_kernel(
         const int bx0 = tx * TBX, by0 = ty * TBY;
         if (tid < NBLK) s_dg[tid] = 0.0f;
         const int py0 = by0 * S, px0 = bx0 * S;
+        // walks the T x PH x PW patch: rows per warp (frame, row and mirrored row warp-uniform),
+        // columns per lane (mirrored column computed once per lane and column group)
+        auto over_patch = [&](auto&& body) {
+            for (int c = lane; c < PW; c += 32) {
+                const int px = px0 + c;
+                const bool cin = px < pw;
+                const int mx = cin ? mirror(px - ox, W) : 0;
+#pragma unroll
+                for (int t = 0; t < T; ++t)
+                    for (int r = warp; r < PH; r += L::NTH / 32) {
+                        const int py = py0 + r;
+                        const bool in = cin && py < ph;
+                        body(t, r, c, in, (long long)(py < ph ? mirror(py - oy, Hh) : 0), mx);
+                    }
+            }
+        };
         __syncthreads();  // tables and the previous tile's flush are complete
-        // the tile's source patch (T frames, PH x PW samples through the mirror), coalesced
-        for (int i = tid; i < T * PH * PW; i += L::NTH) {
-            const int t = i / (PH * PW), rem = i - t * (PH * PW);
-            const int r = rem / PW, c = rem - r * PW;
-            const int py = py0 + r, px = px0 + c;
-            dxp[(t * PH + r) * PP + c] =
-                (py < ph && px < pw)
-                    ? __ldg(job.src[t] + (long long)mirror(py - oy, Hh) * job.src_stride + mirror(px - ox, W))
-                    : 0.0f;
-        }
+        // the tile's source patch through the mirror, coalesced
+        over_patch([&](int t, int r, int c, bool in, long long my, int mx) {
+            dxp[(t * PH + r) * PP + c] = in ? __ldg(job.src[t] + my * job.src_stride + mx) : 0.0f;
+        });
         __syncthreads();
 
         // ---- rows: r2c_x of the windowed source blocks (t < T) and of the
@@ -381,7 +400,8 @@ __global__ void __launch_bounds__(AdjTile<B, T>::NTH, 2) dfttest_adjoint_kernel(
                             const float cs = s_tw[2 * kt], sn = s_tw[2 * kt + 1];
                             const float Gr = hr * cs - hi * sn;
                             const float Gi = hr * sn + hi * cs;
-                            const float wr = s_wf[2 * i], wi = s_wf[2 * i + 1];
+                            const float2 w2 = reinterpret_cast<const float2*>(s_wf)[i];
+                            const float wr = w2.x, wi = w2.y;
                             const float dr = re[kt] - g * wr, di = im[kt] - g * wi;
                             float m, dpsd, dsig;
                             gain_grad<FT>(dr * dr + di * di, s_sig[i], a, m, dpsd, dsig);
@@ -462,14 +482,10 @@ __global__ void __launch_bounds__(AdjTile<B, T>::NTH, 2) dfttest_adjoint_kernel(
         __syncthreads();
 
         // ---- transposed gather: the patch back through the mirror into the source gradients
-        for (int i = tid; i < T * PH * PW; i += L::NTH) {
-            const int t = i / (PH * PW), rem = i - t * (PH * PW);
-            const int r = rem / PW, c = rem - r * PW;
-            const int py = py0 + r, px = px0 + c;
+        over_patch([&](int t, int r, int c, bool in, long long my, int mx) {
             const float v = dxp[(t * PH + r) * PP + c];
-            if (py < ph && px < pw && v != 0.0f)
-                atomicAdd(job.gsrc[t] + (long long)mirror(py - oy, Hh) * job.gsrc_stride + mirror(px - ox, W), v);
-        }
+            if (in && v != 0.0f) atomicAdd(job.gsrc[t] + my * job.gsrc_stride + mx, v);
+        });
     }
 
     // ---- sigma gradient: the CTA's partials -> global
