@@ -29,7 +29,7 @@ pytestmark = pytest.mark.gpu
 
 CANARY = 0xA5
 SHAPES = [(8, 6, 1), (8, 4, 3), (8, 6, 7), (16, 12, 3), (16, 8, 5), (16, 12, 7), (16, 0, 3), (32, 24, 1),
-          (32, 24, 3), (32, 28, 5), (32, 31, 3), (32, 24, 7)]
+          (32, 24, 3), (32, 28, 5), (32, 24, 5), (32, 16, 5), (32, 31, 3), (32, 24, 7)]
 SIZES = [(71, 53), (130, 97)]
 KINDS = [(np.uint8, 0, 8), (np.uint16, 0, 16), (np.float32, 1, 32)]
 GUARD_ROWS = 3

@@ -96,7 +96,8 @@ def test_against_reference_build(cfg, cuda_device):
 
 @pytest.mark.parametrize("B,sosize,tb", [(8, 6, 1), (8, 6, 3), (8, 4, 5), (16, 12, 3), (32, 24, 1), (32, 16, 3),
                                          (16, 8, 1), (32, 24, 5), (32, 24, 7), (32, 24, 3), (32, 28, 3),
-                                         (16, 12, 5), (16, 12, 7), (16, 0, 5), (32, 0, 3), (16, 0, 7)])
+                                         (16, 12, 5), (16, 12, 7), (16, 0, 5), (32, 0, 3), (16, 0, 7),
+                                         (32, 16, 5), (32, 0, 5)])
 @pytest.mark.parametrize("dtype,bits", [(np.float32, 32), (np.uint16, 16)])
 def test_against_fp64_oracle(B, sosize, tb, dtype, bits, cuda_device):
     rng = np.random.default_rng(B + tb)

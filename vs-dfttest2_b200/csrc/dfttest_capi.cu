@@ -110,6 +110,8 @@ using namespace dft2h;
 // global memory, which leaves room for those strips. 16x16x3 runs two 10-warp
 // CTAs per SM (96 registers per thread): 20 warps hide more latency than
 // two 8-warp CTAs at 128 registers (2.5 % faster on the 1080p workload).
+int strip_blocks(const Variant& v, int B, int S);
+
 Variant select_variant(int B, int T, int S) {
     // DFTTEST2_B200_WARPS=16 / 8 / 4 select other 16x16x3 shapes
     const char* env = std::getenv("DFTTEST2_B200_WARPS");
@@ -138,7 +140,21 @@ Variant select_variant(int B, int T, int S) {
         case 1: return unit_variant(32, 1, 16, 1);
         // two 6-warp CTAs per SM unless the overlap needs wider strips (sosize 26 and up)
         case 3: return S >= 7 ? unit_variant(32, 3, 6, 2) : unit_variant(32, 3, 8, 1);
-        case 5: return unit_variant(32, 5, 5, 1);
+        case 5: {
+            // one CTA per SM of 5, 6 or 7 warps: the shape whose strip (as wide as shared memory
+            // allows, at most one block per warp) keeps the most warps busy, the fewest warps on a tie
+            Variant best;
+            int best_w = 0;
+            for (int nw : {5, 6, 7}) {
+                const Variant v = unit_variant(32, 5, nw, 1);
+                const int w = std::min(strip_blocks(v, B, S), nw);
+                if (w > best_w) {
+                    best = v;
+                    best_w = w;
+                }
+            }
+            return best;
+        }
         case 7: return unit_variant(32, 7, 5, 1);
         }
         break;
@@ -176,6 +192,13 @@ std::vector<Variant> candidate_variants(int B, int T, int S) {
         v.push_back(unit_variant(16, 3, 16, 1));
         v.push_back(unit_variant(16, 3, 4, 4));
     }
+    // 32x32x5: the warp buffers (20.5 KB each) and the strip ring share 227 KB; 5, 6 and 7 warps
+    // fit with strips of up to 5 / 6 / 7 blocks (one CTA per SM each)
+    if (B == 32 && T == 5)
+        for (int nw : {7, 6, 5}) {
+            const Variant o = unit_variant(32, 5, nw, 1);
+            if (o.main != v.front().main) v.push_back(o);
+        }
     return v;
 }
 

@@ -10,6 +10,8 @@ Variant unit_variant_b32(int T, int NW, int MINB) {
     DFT2_UNIT_SHAPE(32, 3, 8, 1)
     DFT2_UNIT_SHAPE(32, 3, 4, 2)
     DFT2_UNIT_SHAPE(32, 5, 5, 1)
+    DFT2_UNIT_SHAPE(32, 5, 6, 1)
+    DFT2_UNIT_SHAPE(32, 5, 7, 1)
     DFT2_UNIT_SHAPE(32, 7, 5, 1)
     return Variant{};
 }
