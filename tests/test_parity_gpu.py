@@ -223,10 +223,11 @@ def test_batch_of_planes_matches_single_launches(cuda_device):
     check(batch[5], O.quantize(f64, np.uint16, 16), 16, "batch frame 5")
 
 
-@pytest.mark.parametrize("nframes", [1, 3, 13, 40])
+@pytest.mark.parametrize("nframes", [1, 3, 13, 40, 90])
 def test_multi_plane_host_pipeline_equals_device_path(nframes, cuda_device):
     """dfttest2_b200_process_clip_planes_host (one pipeline over the three
-    planes of a YUV420P16 clip, chunks ramping 4, 12, 32, ..., 12, 4) gives the
+    planes of a YUV420P16 clip, chunks ramping 2, 6, 16, equal chunks of at
+    most 32 frames, then 16, 6, 2) gives the
     device path's result for every frame, including the clip-end clamp
     (within 1 LSB: the launches split planes into units differently, which
     reorders the overlap-add sums at unit edges)."""
