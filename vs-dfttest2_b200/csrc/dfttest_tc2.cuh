@@ -611,13 +611,38 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
                     }
                 }
             }
+            // ---- 4. inverse-y products of block row bb (accumulated into D_out), issued as soon as the
+            //      inverse x of every thread is in shared memory: the barrier of the y-product wait (an
+            //      explicit hand-off when no front half runs) orders them, and they run while the Y
+            //      operand below is written (the tensor cores then run them before the x products)
+            if (back) async_proxy_fence();
             if (front) {
-                // ---- 3. Y operand: lane x writes its (p, j) columns as 16-byte rows (the Y operand
-                //      aliases the gain output, which the inverse x above has consumed)
                 if (!wait_batch(BY)) {
                     failed = true;
                     break;
                 }
+            } else {
+                to_tensor_cores();
+            }
+            if (back && issuer && warp < 2) {  // tile h = warp (an empty commit when the strip has one tile)
+                const int h = warp;
+                if (h < ntile) {
+                    // output row (bb S + y) of the block lands in accumulator column (bb S + y) mod 16:
+                    // the constant's columns are rotated; the unit's first block row starts the sums
+                    const uint32_t id = idesc2(FMT, 128, 16, true, false);
+                    const uint32_t ah = a_ai + h * L.ai_tile;
+                    const uint32_t wi = a_wi + (((bb * S) & 15) / S) * 2 * WY_BYTES;
+                    const uint64_t da = sdesc(0, 128, 256);
+#pragma unroll
+                    for (int part = 0; part < 2; ++part)
+                        mma3(part, tmem + C_OUT + 16 * h, ah, ah + 16 * 256, da, wi, wi + WY_BYTES, da, id,
+                             bb > u.by0);
+                }
+                commit(BIY);
+            }
+            if (front) {
+                // ---- 3. Y operand: lane x writes its (p, j) columns as 16-byte rows (the Y operand
+                //      aliases the gain output, which the inverse x above has consumed)
                 const int x = quarter * 32 + lane;
                 constexpr int CPH = NJ / 2;  // columns per half
                 float v[CPH / 8][8];  // every load issued before one wait
@@ -632,28 +657,9 @@ __global__ void __launch_bounds__(256, 2) dfttest_tc2_kernel(const __grid_consta
                         put_row8<FMT>(dst, dst + L.yb_hl, v[c8]);
                     }
                 }
-            }
-            // ---- 4 and 7. products: inverse y of block row bb (accumulated into D_out), then the x
-            //      products of block row it (D_X, the Y products read above included)
-            to_tensor_cores();
-            if (issuer) {
-                if (back && warp < 2) {  // tile h = warp (an empty commit when the strip has one tile)
-                    const int h = warp;
-                    if (h < ntile) {
-                        // output row (bb S + y) of the block lands in accumulator column (bb S + y) mod 16:
-                        // the constant's columns are rotated; the unit's first block row starts the sums
-                        const uint32_t id = idesc2(FMT, 128, 16, true, false);
-                        const uint32_t ah = a_ai + h * L.ai_tile;
-                        const uint32_t wi = a_wi + (((bb * S) & 15) / S) * 2 * WY_BYTES;
-                        const uint64_t da = sdesc(0, 128, 256);
-#pragma unroll
-                        for (int part = 0; part < 2; ++part)
-                            mma3(part, tmem + C_OUT + 16 * h, ah, ah + 16 * 256, da, wi, wi + WY_BYTES, da, id,
-                                 bb > u.by0);
-                    }
-                    commit(BIY);
-                }
-                if (front) {  // region (tile h, part c) = (warp / 2, warp % 2)
+                // ---- 7. x products of block row it (D_X, the Y products read above included)
+                to_tensor_cores();
+                if (issuer) {  // region (tile h, part c) = (warp / 2, warp % 2)
                     const int h = warp >> 1, c = warp & 1;
                     if (h < ntile) {
                         const uint32_t id = idesc2(FMT, 128, NJ, false, true);
