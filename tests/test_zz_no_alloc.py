@@ -11,8 +11,9 @@ Checked here through the C ABI: two calls in a row, on different inputs,
 each match the regular entry point (dfttest2_b200_process_planes) within the
 parity tolerance of the other GPU tests (1 LSB on integer planes, 2e-5 of
 full scale on float planes); a plane that needs more scratch than the array
-holds is rejected with a clear message; the kernels' error word, read by
-dfttest2_b200_noalloc_check, reports no failure.  This file is collected last so that
+holds is rejected with a clear message, and so is a call inside a stream
+capture; the kernels' error word, read by dfttest2_b200_noalloc_check,
+reports no failure.  This file is collected last so that
 a run stopping at the first failure has already run every other test.
 """
 import ctypes
@@ -144,3 +145,33 @@ def test_noalloc_rejects_planes_beyond_the_array(cuda_device):
     assert "too large for the allocation-free path" in msg
     assert str(_lib.NOALLOC_SCRATCH_BYTES) in msg
     del keep
+
+
+def test_noalloc_rejects_stream_capture(cuda_device):
+    """Inside a stream capture the call is refused (its table copies come from
+    host memory of its own stack frame, which a replayed graph would read
+    after the call returned); the capture itself stays valid."""
+    import torch
+
+    args = plugin_arguments(ftype=0, sigma=8.0, sbsize=16, sosize=12, tbsize=3)
+    lib = _lib.load()
+    p, keep = _params(args)
+    frames = torch.zeros((3, 48, 64), dtype=torch.float32, device=cuda_device)
+    out = torch.empty((48, 64), dtype=torch.float32, device=cuda_device)
+    pl = _plane(frames, 1, 1, out)
+    stream = ctypes.c_void_p(torch.cuda.current_stream(cuda_device).cuda_stream)
+    assert lib.dfttest2_b200_process_plane_noalloc(ctypes.byref(p), ctypes.byref(pl), 1, 32, stream) == 0
+    torch.cuda.synchronize()
+    x = torch.zeros(16, device=cuda_device)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        x.add_(1.0)
+        cs = ctypes.c_void_p(torch.cuda.current_stream(cuda_device).cuda_stream)
+        rc = lib.dfttest2_b200_process_plane_noalloc(ctypes.byref(p), ctypes.byref(pl), 1, 32, cs)
+        msg = lib.dfttest2_b200_last_error().decode()
+    g.replay()
+    torch.cuda.synchronize()
+    assert rc != 0 and "stream capture" in msg
+    assert float(x.sum()) == 16.0
+    assert lib.dfttest2_b200_noalloc_check(0, stream) == 0
+    del g, keep
