@@ -308,11 +308,12 @@ void dfttest2_b200_batch_free(dfttest2_b200_batch* b);
  * rejected with an error that states both sizes.
  *
  * The first call on a device resolves the array's device address.  A call
- * inside a stream capture is rejected (DFTTEST2_B200_EINVAL): the tables and
- * the plane descriptor are copied with cudaMemcpyAsync from pageable host
- * memory of the call's own stack frame, which a replayed graph would read
- * after the call has returned (pageable copies may also wait for the
- * stream).  All calls on a device share the array, so calls that overlap on
+ * inside a stream capture is rejected (DFTTEST2_B200_EINVAL): the plane
+ * descriptor (from the call's stack frame) and the tables (from a
+ * process-wide host buffer that the next call rewrites) are copied with
+ * cudaMemcpyAsync from pageable host memory, which a replayed graph would
+ * read again after the call has returned (pageable copies may also wait for
+ * the stream).  All calls on a device share the array, so calls that overlap on
  * the GPU (different streams, or concurrent host threads) race: serialise
  * them on one stream. */
 int dfttest2_b200_process_plane_noalloc(const dfttest2_b200_params* params, const dfttest2_b200_plane* plane,

@@ -148,9 +148,9 @@ def test_noalloc_rejects_planes_beyond_the_array(cuda_device):
 
 
 def test_noalloc_rejects_stream_capture(cuda_device):
-    """Inside a stream capture the call is refused (its table copies come from
-    host memory of its own stack frame, which a replayed graph would read
-    after the call returned); the capture itself stays valid."""
+    """Inside a stream capture the call is refused (its descriptor and table
+    copies come from host memory that the call does not keep: its stack frame
+    and a buffer the next call rewrites); the capture itself stays valid."""
     import torch
 
     args = plugin_arguments(ftype=0, sigma=8.0, sbsize=16, sosize=12, tbsize=3)

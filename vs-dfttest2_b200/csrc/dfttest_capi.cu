@@ -1886,15 +1886,16 @@ extern "C" int dfttest2_b200_process_plane_noalloc(const dfttest2_b200_params* p
     if (dev != device_id) return fail(DFTTEST2_B200_EINVAL, "invalid device_id");
     CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
     {
-        // the tables and the plane descriptor are copied from this call's stack frame: a captured
-        // copy would read it again at every replay, after the frame is gone
+        // the plane descriptor is copied from this call's stack frame and the tables from a
+        // process-wide host buffer that the next call rewrites: a captured copy would read them
+        // again at every replay, after the frame is gone and the buffer has changed
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         const cudaError_t e = cudaStreamIsCapturing((cudaStream_t)stream, &cs);
         if (e != cudaSuccess) cudaGetLastError();
         if (e != cudaSuccess || cs != cudaStreamCaptureStatusNone)
             return fail(DFTTEST2_B200_EINVAL,
-                        "dfttest2_b200_process_plane_noalloc cannot run inside a stream capture (its table copies "
-                        "come from host memory that ends with the call)");
+                        "dfttest2_b200_process_plane_noalloc cannot run inside a stream capture (its table and "
+                        "descriptor copies come from host memory that the call does not keep)");
     }
 
     const int BPS = strip_blocks(var, B, S);
